@@ -1,0 +1,316 @@
+#!/usr/bin/env python
+"""Benchmark: MPS time steps of the 3D dam break (1,595,308 particles, 1,024,000
+fluid) on B200, through the C-ABI of voxarmps_b200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one full MPS time step (neighbour search, PND, prediction, PPE
+assembly + CG to the stated relative residual, gradient, integration,
+collision, commit).  ``value`` is whole-job particle-steps/s with the state
+resident in HBM; ``e2e`` is the same metric through the public API with host
+buffers (state uploaded from pinned host memory and downloaded every step).
+Under torchrun each rank advances its own copy of the scene (independent
+scenes, no collective on the data path: weak scaling); timings are the max
+over ranks.  ``--impl reference`` times the reference's own CPU path
+(oracle/_ref, OpenMP on all host cores) on a bounded sample of the workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+METRIC = "particle-steps/s"
+# ncu capture of k_cg_spmv (profiles/cg_spmv_dam3d.md): DRAM bytes per launch
+# scaled to the full workload by non-zeros; None until a capture exists.
+SPMV_TRAFFIC_BYTES_PER_NNZ = None
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def peaks():
+    try:
+        with open(PEAKS_FILE) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def spmv_algorithmic_bytes(nnz_a: float, rows: float) -> float:
+    """Bytes one FP64 ELL SpMV must move: per stored non-zero a column index
+    (4 B) and a value (8 B); per unknown row diag (8), length (4), bcon (4),
+    the row's own p (8) and the written s (8).  Gathers of p_j are L2 hits."""
+    return nnz_a * 12.0 + rows * 32.0
+
+
+def build_case():
+    from voxarmps_b200 import config
+    cfg, case = config.baseline(1)
+    cfg = config.solver_semantics(cfg)
+    cfg["cg_tol"] = 1e-8
+    cfg["cg_max"] = 1000
+    return cfg, case
+
+
+def cpu_reference_sample():
+    """Bounded CPU sample: 3D dam at the benchmark's spacing, 10x20x10 fluid in a
+    40x25x10 tank (12,608 particles), single support radius 4.0*l0 (the
+    reference has one radius for every stage)."""
+    from voxarmps_b200 import config
+    cfg, case = config.scaled_dam3d(1)
+    cfg = dict(cfg)
+    cfg["re_s"] = cfg["re_l"] = 4.0 * cfg["l0"]
+    return cfg, case
+
+
+def time_reference(steps: int, warmup: int, nthreads: int):
+    """The reference's own OpenMP CPU path (oracle/_ref/libref_omp.so); if it
+    was not built, the C restatement (single thread) stands in."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    cfg, case = cpu_reference_sample()
+    n = len(case["x"])
+    if pyoracle.ref_available(omp=True):
+        kind, h = "reference", pyoracle.RefHarness(cfg, case, nthreads=nthreads)
+        cores = nthreads
+    else:
+        pyoracle.build()
+        kind, h = "port", pyoracle.Oracle(dict(cfg, solver=0), case)
+        cores = 1
+    h.init()
+    for _ in range(warmup):
+        h.step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        h.step()
+    el = time.perf_counter() - t0
+    h.close()
+    return {"value": n * steps / el, "unit": METRIC, "cores": cores, "kind": kind,
+            "sample": f"3D dam, l0=0.005, re=4.0*l0, {n} particles "
+                      f"(10x20x10 fluid), {steps} steps after {warmup} warm-up",
+            "ms_per_step": el / steps * 1e3}
+
+
+def run_reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    nthreads = os.cpu_count() or 1
+    r = time_reference(args.steps, args.warmup, nthreads)
+    line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": METRIC,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "3D dam break, config-1 spacing and radii, bounded CPU "
+                                   "sample (the full 1.6M-particle case is infeasible on CPU)",
+                       "particles": 12608},
+            "cpu_baseline": {"value": r["value"], "unit": METRIC, "cores": r["cores"],
+                             "kind": r["kind"], "sample": r["sample"]},
+            "e2e": {"value": r["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import voxarmps_b200 as vm
+
+    ws, rank, local = dist_env()
+    dev = local if torch.cuda.device_count() > 1 else 0
+    torch.cuda.set_device(dev)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    cfg, case = build_case()
+    n = len(case["x"])
+    fp = int((case["ptype"] > 0).sum())
+    s = vm.Solver(cfg, case, device=dev)
+    s.init()
+    s.set_profile(True)
+    stream = torch.cuda.ExternalStream(s.stream())
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v: float) -> float:
+        if ws == 1:
+            return v
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        s.step()
+    # ---- device-resident timed region ----
+    s.set_profile(True)
+    iters, ppe_ms = [], []
+    sampler = ClockSampler(dev)
+    barrier()
+    sampler.start()
+    l0 = s.scalar("launches")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    status = 0
+    for _ in range(args.steps):
+        status |= s.step()
+        iters.append(s.scalar("cg_iters"))
+        ppe_ms.append(s.scalar("ms_ppe"))
+    e1.record(stream)
+    barrier()
+    launches = int(s.scalar("launches") - l0)
+    clocks = sampler.stop()
+    el_ms = max_over_ranks(e0.elapsed_time(e1))
+    spmv_ms = s.scalar("spmv_ms")
+    spmv_n = s.scalar("spmv_launches")
+    nnz_a = s.scalar("nnz_a")
+    rows = float((s.get("bcon") == 0).sum())
+    relres = s.scalar("cg_relres")
+    # ---- end-to-end through the API with host buffers ----
+    names = ["x", "y", "z", "u", "v", "w", "p"]
+    host = {k: torch.from_numpy(s.get(k)).pin_memory() for k in names}
+    ptrs = [host[k].data_ptr() for k in names]
+    s.set_profile(False)
+    barrier()
+    t0 = time.perf_counter()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        s.set_state(*ptrs)
+        s.step()
+        s.get_state(*ptrs)
+    e3.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(max(e2.elapsed_time(e3), (time.perf_counter() - t0) * 1e3))
+    bytes_state = 8 * n * len(names)
+    peak, peak_kind = peaks()
+    spmv_avg_ms = spmv_ms / max(spmv_n, 1)
+    algo = spmv_algorithmic_bytes(nnz_a, rows)
+    achieved = algo / (spmv_avg_ms * 1e-3) / 1e9 if spmv_n else None
+    traffic = (SPMV_TRAFFIC_BYTES_PER_NNZ * nnz_a) if SPMV_TRAFFIC_BYTES_PER_NNZ else None
+    line = None
+    if rank == 0:
+        cpu = time_reference(steps=3, warmup=1, nthreads=os.cpu_count() or 1) if ws == 1 else None
+        value = n * args.steps * ws / (el_ms * 1e-3)
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": el_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "3D dam break, 80x160x80 fluid (1,024,000) + 571,308 wall/"
+                                   "dummy particles, l0=0.005, re=2.1/4.0*l0, dt=5e-5, "
+                                   "FP64 Jacobi-PCG to 1e-8 relative residual",
+                       "particles": n, "fluid_particles": fp,
+                       "parallelism": f"{ws} independent scenes" if ws > 1 else "1 scene",
+                       "l2": "working set (lists, matrix) > 126 MB L2; no flush needed"},
+            "fluid_particle_steps_per_s": fp * args.steps * ws / (el_ms * 1e-3),
+            "ppe_ms_per_step": statistics.mean(ppe_ms), "cg_iters_mean": statistics.mean(iters),
+            "cg_relres_last": relres, "status_bits": status,
+            "roofline": {"kernel": "k_cg_spmv (PPE SpMV, FP64 slot-major ELL)", "bound": "hbm",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None,
+                         "traffic": traffic, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": algo,
+                         "avg_launch_ms": spmv_avg_ms, "launches_timed": int(spmv_n)},
+            "e2e": {"value": n * args.steps * ws / (e2e_ms * 1e-3), "unit": METRIC,
+                    "h2d_bytes_per_step": bytes_state, "d2h_bytes_per_step": bytes_state},
+            "gpu_launches": launches, "clocks": clocks,
+            "cpu_baseline": ({k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+                             if cpu else None),
+        }
+    s.close()
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if line:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

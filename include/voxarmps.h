@@ -1,0 +1,157 @@
+/*
+ * voxarmps.h -- C-ABI of the Blackwell-native (sm_100a) MPS solver core.
+ *
+ * Drop-in for the per-step entry points of VoxarMPS (declared in
+ * VoxarMPS/VoxarMPS/functions.cuh:56-111 and driven by main.cu:1027-1363).
+ * The reference passes 1-based host arrays to free functions that mutate
+ * them; here a context owns every device buffer, the caller's host arrays
+ * are borrowed only for the duration of a call, and every call returns a
+ * status code instead of printing (functions.cu:2720-2743) or exit()ing.
+ *
+ * Particle arrays crossing this boundary are 0-based and in the caller's
+ * particle order (the reference's id order).  Inside the context particles
+ * live in cell order; downloads translate back.
+ *
+ * Thread safety: one context per host thread / stream; no global state.
+ */
+#ifndef VOXARMPS_H
+#define VOXARMPS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (bit flags; a call may return several) ---------------- */
+#define MPS_OK 0
+#define MPS_ERR_ARG 1             /* bad argument / call order */
+#define MPS_ERR_CUDA 2            /* CUDA runtime error (message: mps_last_message) */
+#define MPS_ERR_NAN 4             /* non-finite p/u/v/w, reference ERROR#1 (functions.cu:2720) */
+#define MPS_ERR_BOX 8             /* particle at/outside the box, ERROR#2 (functions.cu:2725) */
+#define MPS_ERR_CELL 16           /* particle outside the cell grid (unchecked in NEIGHBOR) */
+#define MPS_ERR_LIST_OVERFLOW 32  /* a neighbour list exceeded its capacity (inOut.h:30) */
+#define MPS_ERR_NOT_CONVERGED 64  /* PPE did not reach cg_tol within cg_max iterations */
+#define MPS_ERR_IO 128            /* file could not be read / written */
+
+/* ---- configuration ------------------------------------------------------ *
+ * Every constant main.cu hard-codes (main.cu:211-394) is a field.  The
+ * Python mirror is voxarmps_b200.config.FIELDS (same order). */
+typedef struct mps_config {
+    int dim;              /* 2 or 3 (main.cu:186) */
+    int ktype;            /* kernel function type 1,2,3,5,6 (functions.cu:32-74) */
+    int method;           /* 1 fully incompressible PPE, 3 weakly compressible (main.cu:338) */
+    double l0;            /* particle spacing DL */
+    double re_s;          /* PND / gradient / collision support radius */
+    double re_l;          /* Laplacian (PPE, viscous term) support radius */
+    double delta;         /* DELTA: 3D z-cell expansion and 3D cutoff slack (main.cu:283) */
+    double dt;
+    double gx, gy, gz;
+    double rho1, rho2, nu1, nu2;
+    double beta_fs;       /* WC free-surface threshold */
+    double dirichlet;     /* free surface where n_star / n0 < dirichlet (main.cu:226) */
+    double relaxp;
+    int kh;               /* Khayyer-Gotoh pressure-gradient correction */
+    double vmax;
+    double coll;          /* collision distance */
+    double cc;            /* collision restitution coefficient */
+    double velcor;        /* wall reflection factor (main.cu:1293) */
+    double ncorrection;   /* PND correction for ktype != 2 */
+    double pmin, pmax;
+    double c01, c02;      /* WC sound speeds */
+    int turb;             /* SPS-LES turbulence */
+    double cs;            /* Smagorinsky constant */
+    int fluid2_type;      /* 0 Newtonian, 1 Herschel-Bulkley second fluid */
+    double n_pl, meu0, phi, cohes;
+    int matopt, srcopt;   /* HL Laplacian, HS+ECS source */
+    int fraction_method;  /* 1 linear, 2 kernel-smoothed */
+    int ppe_at_predicted; /* 1: A at x*, b from n* (reference GPU path); 0: CPU path */
+    int warm_start;       /* 1: CG starts from the previous pressure */
+    int solver;           /* 1 Jacobi-PCG, 2 unpreconditioned CG (relative residual) */
+    double cg_tol;        /* relative residual ||b-Ax||/||b|| */
+    int cg_max;
+    int imin, imax;       /* kept for layout parity with the oracle; unused here */
+    double eps;
+    int collision_gather; /* must be 1: order-independent collision */
+    double xmin, xmax, ymin, ymax, zmin, zmax;  /* grown bounding box (main.cu:692-715) */
+    /* B200 path knobs (no reference counterpart) */
+    int precision;        /* 0 FP64 throughout; 1 mixed (FP32 streams + FP64 refinement) */
+    int list_cap_s;       /* neighbour-list capacity per particle, 0 = automatic */
+    int list_cap_l;
+} mps_config;
+
+typedef struct mps_ctx mps_ctx;
+
+/* Lifecycle.  Replaces main.cu's allocation block (main.cu:726-921). */
+int mps_create(const mps_config* cfg, int device, mps_ctx** out);
+int mps_destroy(mps_ctx* ctx);
+
+/* Host -> device particle upload (main.cu:947-962).  z, w may be NULL in
+ * 2D; u, v, w, p may be NULL (zero).  Arrays are borrowed for the call. */
+int mps_upload(mps_ctx* ctx, int n, const double* x, const double* y, const double* z,
+               const int* ptype, const double* u, const double* v, const double* w,
+               const double* p);
+/* Read a .grd file (main.cu:496-684 format) and upload it. */
+int mps_load_grd(mps_ctx* ctx, const char* path);
+
+/* Pre-iteration work (main.cu:964-1012): density, lists, n0 = max PND. */
+int mps_init(mps_ctx* ctx);
+
+/* Per-stage entry points, one per reference routine, in main.cu's order. */
+int mps_pnd(mps_ctx* ctx);                /* PNUM           functions.cu:94   */
+int mps_neighbors(mps_ctx* ctx);          /* NEIGHBOR       functions.cu:2788 */
+int mps_sps(mps_ctx* ctx);                /* SPS            functions.cu:1719 */
+int mps_vfraction(mps_ctx* ctx);          /* V_FRACTION     functions.cu:2580 */
+int mps_viscosity(mps_ctx* ctx);          /* VISCOSITY      functions.cu:2053 */
+int mps_predict(mps_ctx* ctx);            /* PREDICTION     functions.cu:2283 */
+int mps_pnd_star(mps_ctx* ctx);           /* PNUMSTAR       functions.cu:157  */
+int mps_bcon(mps_ctx* ctx);               /* BCON           functions.cu:433  */
+int mps_pressure(mps_ctx* ctx, int* iters, double* relres); /* PRESSURECALC functions.cu:2465 */
+int mps_phat(mps_ctx* ctx);               /* PHATCALC       functions.cu:207  */
+int mps_pressure_gradient(mps_ctx* ctx);  /* PRESSGRAD      functions.cu:245  */
+int mps_integrate(mps_ctx* ctx);          /* EULERINTEGRATION functions.cu:2004 */
+int mps_collision(mps_ctx* ctx);          /* COLLISION2     functions.cu:1523 */
+int mps_commit(mps_ctx* ctx);             /* PREPDATA       functions.cu:2688 */
+
+/* One full time step (main.cu:1027-1349 loop body) / several steps. */
+int mps_step(mps_ctx* ctx);
+int mps_run(mps_ctx* ctx, int steps);
+
+/* Device -> host.  Field names: x y z u v w p pnew phat un vn wn xs ys zs us vs
+ * ws n nstar C meu neut t1 t2 t3 rho source diag (double); ptype bcon (int);
+ * cell_s cell_l (int, 1-based Cnum per particle, NEIGHBOR's cell number);
+ * perm_s perm_l (int, particle ids in cell order: NEIGHBOR's ip[]).
+ * Returns MPS_OK; *count (optional) receives the element count. */
+int mps_download(mps_ctx* ctx, const char* field, void* out, long* count);
+/* Neighbour lists in particle-id space, CSR: which 0 = PND radius, 1 =
+ * Laplacian radius.  off has n+1 entries; nbr needs off[n] (query with
+ * nbr == NULL first: *total receives the entry count). */
+int mps_download_lists(mps_ctx* ctx, int which, int* off, int* nbr, long* total);
+/* Overwrite / read the particle state between steps, host arrays in the
+ * caller's particle order (the reference keeps x..p in caller-owned host
+ * arrays across steps, main.cu:554-563).  NULL arrays are skipped; set_state
+ * also sets pnew = p as PREPDATA leaves it (functions.cu:2700). */
+int mps_set_state(mps_ctx* ctx, const double* x, const double* y, const double* z,
+                  const double* u, const double* v, const double* w, const double* p);
+int mps_get_state(mps_ctx* ctx, double* x, double* y, double* z, double* u, double* v,
+                  double* w, double* p);
+/* Per-stage device timing with CUDA events (off by default).  While on,
+ * scalars ms_neighbors ms_explicit ms_ppe ms_post ms_step (last step) and
+ * spmv_ms / spmv_launches, lists_ms (accumulated) are available. */
+int mps_set_profile(mps_ctx* ctx, int on);
+/* Scalars: n0_s n0_l lambda_l cg_iters cg_relres n nnz_s nnz_l nnz_a steps
+ * cap_s cap_l len_max_s len_max_l launches pmax and the profile timings. */
+int mps_get_scalar(mps_ctx* ctx, const char* name, double* out);
+/* Accumulated MPS_ERR_* bits since the last call (then cleared). */
+int mps_get_error(mps_ctx* ctx);
+const char* mps_last_message(mps_ctx* ctx);
+/* VTU writer (inOut.cpp:104-336 format, ASCII UnstructuredGrid). */
+int mps_write_vtu(mps_ctx* ctx, const char* path, int fluid_only);
+
+/* Device stream the context launches on (cudaStream_t as void*). */
+void* mps_stream(mps_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

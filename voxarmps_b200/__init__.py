@@ -1,1 +1,250 @@
-"""voxarmps_b200 -- Blackwell-native MPS solver core (sm_100a)."""
+"""voxarmps_b200 -- Blackwell-native (sm_100a) MPS solver core.
+
+Python host-side mirror of the C-ABI in include/voxarmps.h.  ``Solver``
+exposes one method per reference stage (NEIGHBOR, PNUM, ... PREPDATA of
+VoxarMPS/VoxarMPS/functions.cuh) plus ``step()`` for main.cu's whole loop
+body.  The CUDA library is required: there is no CPU path, and importing
+``Solver`` on a machine without the built library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import cases, config  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvoxarmps_b200.so")
+
+MPS_OK = 0
+MPS_ERR_ARG = 1
+MPS_ERR_CUDA = 2
+MPS_ERR_NAN = 4
+MPS_ERR_BOX = 8
+MPS_ERR_CELL = 16
+MPS_ERR_LIST_OVERFLOW = 32
+MPS_ERR_NOT_CONVERGED = 64
+MPS_ERR_IO = 128
+FATAL = MPS_ERR_ARG | MPS_ERR_CUDA | MPS_ERR_IO
+
+_CT = {"i": C.c_int, "d": C.c_double}
+
+
+class MpsConfig(C.Structure):
+    """ctypes mirror of ``mps_config``."""
+    _fields_ = [(name, _CT[t]) for name, t in config.FIELDS]
+
+
+EXPORTS = [
+    "mps_create", "mps_destroy", "mps_upload", "mps_load_grd", "mps_init", "mps_pnd",
+    "mps_neighbors", "mps_sps", "mps_vfraction", "mps_viscosity", "mps_predict",
+    "mps_pnd_star", "mps_bcon", "mps_pressure", "mps_phat", "mps_pressure_gradient",
+    "mps_integrate", "mps_collision", "mps_commit", "mps_step", "mps_run", "mps_download",
+    "mps_download_lists", "mps_get_scalar", "mps_get_error", "mps_last_message",
+    "mps_write_vtu", "mps_stream", "mps_set_state", "mps_get_state", "mps_set_profile",
+]
+
+_LIB = None
+
+
+class MpsError(RuntimeError):
+    def __init__(self, code, msg=""):
+        super().__init__(f"voxarmps error {code}: {msg}")
+        self.code = code
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the CUDA library (fails loudly when it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with python -m voxarmps_b200.build")
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    DP = C.POINTER(C.c_double)
+    IP = C.POINTER(C.c_int)
+    lib.mps_create.argtypes = [C.POINTER(MpsConfig), C.c_int, C.POINTER(P)]
+    lib.mps_destroy.argtypes = [P]
+    lib.mps_upload.argtypes = [P, C.c_int, DP, DP, DP, IP, DP, DP, DP, DP]
+    lib.mps_load_grd.argtypes = [P, C.c_char_p]
+    for name in ("mps_init", "mps_pnd", "mps_neighbors", "mps_sps", "mps_vfraction",
+                 "mps_viscosity", "mps_predict", "mps_pnd_star", "mps_bcon", "mps_phat",
+                 "mps_pressure_gradient", "mps_integrate", "mps_collision", "mps_commit",
+                 "mps_step", "mps_get_error"):
+        getattr(lib, name).argtypes = [P]
+    lib.mps_pressure.argtypes = [P, IP, DP]
+    lib.mps_run.argtypes = [P, C.c_int]
+    lib.mps_download.argtypes = [P, C.c_char_p, P, C.POINTER(C.c_long)]
+    lib.mps_download_lists.argtypes = [P, C.c_int, IP, IP, C.POINTER(C.c_long)]
+    lib.mps_get_scalar.argtypes = [P, C.c_char_p, DP]
+    lib.mps_last_message.argtypes = [P]
+    lib.mps_last_message.restype = C.c_char_p
+    lib.mps_write_vtu.argtypes = [P, C.c_char_p, C.c_int]
+    lib.mps_stream.argtypes = [P]
+    lib.mps_stream.restype = P
+    lib.mps_set_state.argtypes = [P, P, P, P, P, P, P, P]
+    lib.mps_get_state.argtypes = [P, P, P, P, P, P, P, P]
+    lib.mps_set_profile.argtypes = [P, C.c_int]
+    _LIB = lib
+    return lib
+
+
+INT_FIELDS = {"ptype", "bcon", "cell_s", "cell_l", "perm_s", "perm_l"}
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+class Solver:
+    """One simulation on one GPU (a context of the C-ABI)."""
+
+    def __init__(self, cfg: dict, case: dict | None = None, device: int = 0):
+        self.lib = load_library()
+        self.cfg = dict(config.reference_defaults(cfg.get("l0", 0.01), cfg.get("dim", 2)))
+        self.cfg.update(cfg)
+        self._c = MpsConfig(**{k: self.cfg[k] for k, _ in config.FIELDS})
+        self.h = C.c_void_p()
+        self._chk(self.lib.mps_create(C.byref(self._c), device, C.byref(self.h)), "create")
+        if case is not None:
+            self.upload(case)
+
+    def _chk(self, r, what=""):
+        if r & FATAL:
+            msg = self.lib.mps_last_message(self.h).decode() if self.h else ""
+            raise MpsError(r, f"{what}: {msg}")
+        return r
+
+    def upload(self, case: dict):
+        n = len(case["x"])
+        f64 = lambda k: np.ascontiguousarray(case[k], np.float64) if k in case else None
+        self._keep = [f64(k) for k in ("x", "y", "z", "u", "v", "w", "p")]
+        pt = np.ascontiguousarray(case["ptype"], np.int32)
+        x, y, z, u, v, w, p = self._keep
+        self._chk(self.lib.mps_upload(self.h, n, _dp(x), _dp(y), _dp(z),
+                                      pt.ctypes.data_as(C.POINTER(C.c_int)), _dp(u), _dp(v),
+                                      _dp(w), _dp(p)), "upload")
+        self.n = n
+        return self
+
+    def load_grd(self, path: str):
+        self._chk(self.lib.mps_load_grd(self.h, path.encode()), "load_grd")
+        self.n = int(self.scalar("n"))
+        return self
+
+    # ---- stages, one per reference routine (functions.cuh:56-111) ----
+    def init(self):
+        return self._chk(self.lib.mps_init(self.h), "init")
+
+    def neighbors(self):
+        return self._chk(self.lib.mps_neighbors(self.h), "neighbors")
+
+    def pnd(self):
+        return self._chk(self.lib.mps_pnd(self.h), "pnd")
+
+    def sps(self):
+        return self._chk(self.lib.mps_sps(self.h), "sps")
+
+    def vfraction(self):
+        return self._chk(self.lib.mps_vfraction(self.h), "vfraction")
+
+    def viscosity(self):
+        return self._chk(self.lib.mps_viscosity(self.h), "viscosity")
+
+    def predict(self):
+        return self._chk(self.lib.mps_predict(self.h), "predict")
+
+    def pnd_star(self):
+        return self._chk(self.lib.mps_pnd_star(self.h), "pnd_star")
+
+    def bcon(self):
+        return self._chk(self.lib.mps_bcon(self.h), "bcon")
+
+    def pressure(self):
+        it, rr = C.c_int(), C.c_double()
+        self._chk(self.lib.mps_pressure(self.h, C.byref(it), C.byref(rr)), "pressure")
+        return it.value, rr.value
+
+    def phat(self):
+        return self._chk(self.lib.mps_phat(self.h), "phat")
+
+    def pressure_gradient(self):
+        return self._chk(self.lib.mps_pressure_gradient(self.h), "pressure_gradient")
+
+    def integrate(self):
+        return self._chk(self.lib.mps_integrate(self.h), "integrate")
+
+    def collision(self):
+        return self._chk(self.lib.mps_collision(self.h), "collision")
+
+    def commit(self):
+        return self._chk(self.lib.mps_commit(self.h), "commit")
+
+    # the reference's routine names
+    NEIGHBOR, PNUM, SPS, V_FRACTION, VISCOSITY = neighbors, pnd, sps, vfraction, viscosity
+    PREDICTION, PNUMSTAR, BCON, PRESSURECALC = predict, pnd_star, bcon, pressure
+    PHATCALC, PRESSGRAD, EULERINTEGRATION, COLLISION2, PREPDATA = (
+        phat, pressure_gradient, integrate, collision, commit)
+
+    def step(self):
+        """One time step (main.cu:1027-1349); returns the MPS_ERR_* bits."""
+        return self._chk(self.lib.mps_step(self.h), "step")
+
+    def run(self, steps: int):
+        return self._chk(self.lib.mps_run(self.h, steps), "run")
+
+    # ---- data out ----
+    def get(self, name: str) -> np.ndarray:
+        out = np.empty(self.n, np.int32 if name in INT_FIELDS else np.float64)
+        self._chk(self.lib.mps_download(self.h, name.encode(), out.ctypes.data_as(C.c_void_p),
+                                        None), f"download {name}")
+        return out
+
+    def lists(self, which: int):
+        """(off, nbr) CSR in particle-id space; which 0 = PND radius, 1 = Laplacian."""
+        tot = C.c_long()
+        self._chk(self.lib.mps_download_lists(self.h, which, None, None, C.byref(tot)), "lists")
+        off = np.empty(self.n + 1, np.int32)
+        nbr = np.empty(max(tot.value, 1), np.int32)
+        IP = C.POINTER(C.c_int)
+        self._chk(self.lib.mps_download_lists(self.h, which, off.ctypes.data_as(IP),
+                                              nbr.ctypes.data_as(IP), C.byref(tot)), "lists")
+        return off, nbr[: tot.value]
+
+    def set_state(self, *ptrs):
+        """Host pointers (ints) for x, y, z, u, v, w, p in caller order; 0 skips."""
+        return self._chk(self.lib.mps_set_state(self.h, *[p or None for p in ptrs]), "set_state")
+
+    def get_state(self, *ptrs):
+        return self._chk(self.lib.mps_get_state(self.h, *[p or None for p in ptrs]), "get_state")
+
+    def set_profile(self, on: bool = True):
+        return self._chk(self.lib.mps_set_profile(self.h, int(on)), "profile")
+
+    def scalar(self, name: str) -> float:
+        v = C.c_double()
+        self._chk(self.lib.mps_get_scalar(self.h, name.encode(), C.byref(v)), f"scalar {name}")
+        return v.value
+
+    def error(self) -> int:
+        return self.lib.mps_get_error(self.h)
+
+    def write_vtu(self, path: str, fluid_only: bool = False):
+        return self._chk(self.lib.mps_write_vtu(self.h, path.encode(), int(fluid_only)), "vtu")
+
+    def stream(self) -> int:
+        return self.lib.mps_stream(self.h) or 0
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.lib.mps_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -28,6 +28,7 @@ FIELDS = [
     ("cg_tol", "d"), ("cg_max", "i"), ("imin", "i"), ("imax", "i"), ("eps", "d"),
     ("collision_gather", "i"),
     ("xmin", "d"), ("xmax", "d"), ("ymin", "d"), ("ymax", "d"), ("zmin", "d"), ("zmax", "d"),
+    ("precision", "i"), ("list_cap_s", "i"), ("list_cap_l", "i"),
 ]
 
 
@@ -49,6 +50,7 @@ def reference_defaults(dl: float, dim: int, compressible: bool = False) -> dict:
         ppe_at_predicted=0, warm_start=0, solver=0, cg_tol=1e-8, cg_max=2000,
         imin=10, imax=50, eps=1.0e-9, collision_gather=0,
         xmin=0.0, xmax=0.0, ymin=0.0, ymax=0.0, zmin=0.0, zmax=0.0,
+        precision=0, list_cap_s=0, list_cap_l=0,
     )
     return cfg
 

@@ -1,0 +1,757 @@
+// mps_context.cu -- the C-ABI (include/voxarmps.h): context lifecycle,
+// device memory, host<->device transfers in the caller's particle order,
+// the step driver in main.cu's stage order, .grd input and VTU output.
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "mps_internal.cuh"
+
+using namespace vmps;
+
+static std::atomic<long long> g_launches{0};
+int vmps_count_launch(int k)
+{
+    g_launches += k;
+    return 0;
+}
+
+int vmps_check(mps_ctx* ctx, cudaError_t e, const char* what)
+{
+    if (e == cudaSuccess) return MPS_OK;
+    if (ctx) ctx->msg = std::string(what) + ": " + cudaGetErrorString(e);
+    return MPS_ERR_CUDA;
+}
+
+namespace {
+
+template <typename T>
+int dalloc(mps_ctx* c, T** p, size_t count)
+{
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, (count > 0 ? count : 1) * sizeof(T));
+    if (e != cudaSuccess) return vmps_check(c, e, "cudaMalloc");
+    e = cudaMemsetAsync(q, 0, (count > 0 ? count : 1) * sizeof(T), c->stream);
+    if (e != cudaSuccess) return vmps_check(c, e, "cudaMemsetAsync");
+    c->owned.push_back(q);
+    *p = (T*)q;
+    return MPS_OK;
+}
+
+template <typename T>
+int halloc(mps_ctx* c, T** p, size_t count)
+{
+    void* q = nullptr;
+    cudaError_t e = cudaMallocHost(&q, (count > 0 ? count : 1) * sizeof(T));
+    if (e != cudaSuccess) return vmps_check(c, e, "cudaMallocHost");
+    memset(q, 0, (count > 0 ? count : 1) * sizeof(T));
+    c->pinned.push_back(q);
+    *p = (T*)q;
+    return MPS_OK;
+}
+
+void free_all(mps_ctx* c)
+{
+    if (c->device >= 0) cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (void* q : c->owned) cudaFree(q);
+    for (void* q : c->pinned) cudaFreeHost(q);
+    c->owned.clear();
+    c->pinned.clear();
+    c->alts.clear();
+}
+
+// NEIGHBOR's grid (functions.cu:2790-2802)
+Grid make_grid(const mps_config& f, double re)
+{
+    Grid g;
+    g.re = re;
+    g.rez = f.dim == 3 ? re + f.delta : re;
+    g.xmin = f.xmin;
+    g.ymin = f.ymin;
+    g.zmin = f.zmin;
+    g.ncx = (int)((f.xmax - f.xmin) / (re)) + 1;
+    g.ncy = (int)((f.ymax - f.ymin) / (re)) + 1;
+    g.ncz = f.dim == 3 ? (int)((f.zmax - f.zmin) / (re + f.delta)) + 1 : 1;
+    g.tnc = g.ncx * g.ncy * g.ncz;
+    return g;
+}
+
+// 2D: sqrt(d2) < re  <=>  d2 < cut  (cut = least d2 with sqrt(d2) >= re).
+// 3D: sqrt(d2) <= c  <=>  d2 <= cut (cut = greatest d2 with sqrt(d2) <= c).
+// sqrt is correctly rounded on the host and on the device, so both sides
+// take identical decisions.
+double sqrt_cut(double c, bool strict)
+{
+    double s = c * c;
+    if (strict) {
+        while (std::sqrt(s) < c) s = std::nextafter(s, INFINITY);
+        while (s > 0 && std::sqrt(std::nextafter(s, 0.0)) >= c) s = std::nextafter(s, 0.0);
+    } else {
+        while (std::sqrt(s) > c) s = std::nextafter(s, 0.0);
+        while (std::sqrt(std::nextafter(s, INFINITY)) <= c) s = std::nextafter(s, INFINITY);
+    }
+    return s;
+}
+
+int lattice_count(int dim, double ratio, bool inclusive)
+{
+    int r = (int)std::ceil(ratio) + 1, cnt = 0;
+    double lim = ratio * ratio;
+    for (int a = -r; a <= r; a++)
+        for (int b = -r; b <= r; b++)
+            for (int k = (dim == 3 ? -r : 0); k <= (dim == 3 ? r : 0); k++) {
+                double d2 = (double)a * a + (double)b * b + (double)k * k;
+                if (inclusive ? d2 <= lim : d2 < lim) cnt++;
+            }
+    return cnt;
+}
+
+int auto_cap(const mps_config& f, double re)
+{
+    bool three = f.dim == 3;
+    double ratio = (three ? re + f.delta : re) / f.l0;
+    int c = lattice_count(f.dim, ratio, three);
+    int cap = (int)std::ceil(c * 1.5) + 8;
+    return (cap + 7) / 8 * 8;
+}
+
+int validate(const mps_config& f, std::string& why)
+{
+    if (f.dim != 2 && f.dim != 3) { why = "dim must be 2 or 3"; return MPS_ERR_ARG; }
+    if (f.method != 1 && f.method != 3) { why = "method must be 1 or 3"; return MPS_ERR_ARG; }
+    if (!(f.l0 > 0) || !(f.re_s > 0) || !(f.re_l > 0) || !(f.dt > 0)) {
+        why = "l0, re_s, re_l and dt must be positive";
+        return MPS_ERR_ARG;
+    }
+    if (f.ktype != 1 && f.ktype != 2 && f.ktype != 3 && f.ktype != 5 && f.ktype != 6) {
+        why = "ktype must be 1, 2, 3, 5 or 6";
+        return MPS_ERR_ARG;
+    }
+    if (f.solver != 1 && f.solver != 2) { why = "solver must be 1 (Jacobi-PCG) or 2 (CG)"; return MPS_ERR_ARG; }
+    if (f.precision != 0) { why = "precision 1 (mixed) is not available in this build"; return MPS_ERR_ARG; }
+    return MPS_OK;
+}
+
+__global__ void k_unpermute_d(int n, const int* __restrict__ oid, const double* __restrict__ a,
+                              double* __restrict__ out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[oid[i]] = a[i];
+}
+
+__global__ void k_unpermute_i(int n, const int* __restrict__ oid, const int* __restrict__ a,
+                              int* __restrict__ out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[oid[i]] = a[i];
+}
+
+__global__ void k_perm_ids(int n, const int* __restrict__ oid, const int* __restrict__ slots,
+                           int* __restrict__ out)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) out[k] = slots ? oid[slots[k]] : oid[k];
+}
+
+__global__ void k_permute_in(int n, const int* __restrict__ oid, const double* __restrict__ in,
+                             double* __restrict__ a, double* __restrict__ b)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v = in[oid[i]];
+    a[i] = v;
+    if (b) b[i] = v;
+}
+
+__global__ void k_iota(int n, int* a)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = i;
+}
+
+__global__ void k_density(int n, const int* __restrict__ ptype, double rho1, double rho2,
+                          double* __restrict__ rho)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) rho[i] = (ptype[i] == 2) ? rho2 : rho1;
+}
+
+int collect_errors(mps_ctx* c)
+{
+    VMPS_CUDA(c, cudaMemcpyAsync(c->h_err, c->d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                                 c->stream));
+    VMPS_CUDA(c, cudaMemsetAsync(c->d_err, 0, sizeof(unsigned int), c->stream));
+    VMPS_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->host_err |= *c->h_err;
+    return (int)(*c->h_err);
+}
+
+int device_max(mps_ctx* c, double* out)
+{
+    unsigned long long h = 0;
+    VMPS_CUDA(c, cudaMemcpyAsync(&h, c->d_max, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    VMPS_CUDA(c, cudaStreamSynchronize(c->stream));
+    double d;
+    memcpy(&d, &h, sizeof(d));
+    *out = d;
+    return MPS_OK;
+}
+
+#define TRY(x)                     \
+    do {                           \
+        int _r = (x);              \
+        if (_r != MPS_OK) return _r; \
+    } while (0)
+
+int allocate(mps_ctx* c)
+{
+    const size_t P = (size_t)c->pitch;
+    double** dfields[] = {&c->x, &c->y, &c->z, &c->u, &c->v, &c->w, &c->p, &c->pnew,
+                          &c->phat, &c->un, &c->vn, &c->wn, &c->rho, &c->nd, &c->xs, &c->ys,
+                          &c->zs, &c->us, &c->vs, &c->ws, &c->nds, &c->C, &c->meu, &c->neut,
+                          &c->t1, &c->t2, &c->t3, &c->source, &c->diag, &c->cg_r, &c->cg_z,
+                          &c->cg_p, &c->cg_s, &c->xc, &c->yc, &c->zc, &c->uc, &c->vc, &c->wc};
+    for (auto f : dfields) TRY(dalloc(c, f, P));
+    int** ifields[] = {&c->ptype, &c->oid, &c->bcon, &c->cell_l, &c->cell_s, &c->bpos_l,
+                       &c->bpos_s, &c->bslot_l, &c->boid_l, &c->bslot_s, &c->boid_s, &c->src,
+                       &c->inv, &c->perm_s, &c->perm_s_tmp, &c->len_l, &c->len_s, &c->mlen};
+    for (auto f : ifields) TRY(dalloc(c, f, P));
+    TRY(dalloc(c, &c->S6, 6 * P));
+    TRY(dalloc(c, &c->stage_in, P));
+    TRY(dalloc(c, &c->cnt_l, (size_t)c->gl.tnc + 2));
+    TRY(dalloc(c, &c->cst_l, (size_t)c->gl.tnc + 2));
+    TRY(dalloc(c, &c->cnt_s, (size_t)c->gs.tnc + 2));
+    TRY(dalloc(c, &c->cst_s, (size_t)c->gs.tnc + 2));
+    size_t tiles = (size_t)std::max(c->gl.tnc, c->gs.tnc) / 8192 + 4;
+    TRY(dalloc(c, &c->scan_tmp, tiles));
+    TRY(dalloc(c, &c->nbr_l, (size_t)c->cap_l * P));
+    TRY(dalloc(c, &c->nbr_s, (size_t)c->cap_s * P));
+    TRY(dalloc(c, &c->mcol, (size_t)c->cap_l * P));
+    TRY(dalloc(c, &c->mval, (size_t)c->cap_l * P));
+    int sms = 0;
+    VMPS_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    TRY(dalloc(c, &c->cg_part, (size_t)8 * 4 * sms + 64));
+    TRY(dalloc(c, &c->cg_scal, 16));
+    TRY(dalloc(c, &c->cg_flag, 4));
+    TRY(dalloc(c, &c->d_err, 1));
+    TRY(dalloc(c, &c->len_max, 2));
+    TRY(dalloc(c, &c->d_max, 1));
+    TRY(halloc(c, &c->cg_flag_host, 4));
+    TRY(halloc(c, &c->red_host, 16));
+    TRY(halloc(c, &c->h_err, 1));
+    // alternates of the persistent fields for the reorder (same order as
+    // persistent_set in mps_neighbors.cu: 14 doubles then 4 ints)
+    c->alts.clear();
+    for (int k = 0; k < 14; k++) {
+        double* q;
+        TRY(dalloc(c, &q, P));
+        c->alts.push_back(q);
+    }
+    for (int k = 0; k < 4; k++) {
+        int* q;
+        TRY(dalloc(c, &q, P));
+        c->alts.push_back(q);
+    }
+    return MPS_OK;
+}
+
+double* field_d(mps_ctx* c, const std::string& f)
+{
+    struct { const char* n; double* p; } t[] = {
+        {"x", c->x}, {"y", c->y}, {"z", c->z}, {"u", c->u}, {"v", c->v}, {"w", c->w},
+        {"p", c->p}, {"pnew", c->pnew}, {"phat", c->phat}, {"un", c->un}, {"vn", c->vn},
+        {"wn", c->wn}, {"xs", c->xs}, {"ys", c->ys}, {"zs", c->zs}, {"us", c->us},
+        {"vs", c->vs}, {"ws", c->ws}, {"n", c->nd}, {"nstar", c->nds}, {"C", c->C},
+        {"meu", c->meu}, {"neut", c->neut}, {"t1", c->t1}, {"t2", c->t2}, {"t3", c->t3},
+        {"rho", c->rho}, {"source", c->source}, {"diag", c->diag}};
+    for (auto& e : t)
+        if (f == e.n) return e.p;
+    return nullptr;
+}
+
+}  // namespace
+
+std::vector<void*>& vmps_reorder_alts(mps_ctx* ctx) { return ctx->alts; }
+
+// ------------------------------------------------------------------ C-ABI
+
+extern "C" {
+
+int mps_create(const mps_config* cfg, int device, mps_ctx** out)
+{
+    if (!cfg || !out) return MPS_ERR_ARG;
+    *out = nullptr;
+    std::string why;
+    int r = validate(*cfg, why);
+    if (r != MPS_OK) {
+        fprintf(stderr, "voxarmps: %s\n", why.c_str());
+        return r;
+    }
+    mps_ctx* c = new mps_ctx();
+    c->cfg = *cfg;
+    c->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "voxarmps: %s\n", cudaGetErrorString(e));
+        delete c;
+        return MPS_ERR_CUDA;
+    }
+    *out = c;
+    return MPS_OK;
+}
+
+int mps_destroy(mps_ctx* c)
+{
+    if (!c) return MPS_OK;
+    free_all(c);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : c->ev_spmv) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return MPS_OK;
+}
+
+int mps_upload(mps_ctx* c, int n, const double* x, const double* y, const double* z,
+               const int* ptype, const double* u, const double* v, const double* w,
+               const double* p)
+{
+    if (!c || n <= 0 || !x || !y || !ptype || (c->cfg.dim == 3 && !z)) return MPS_ERR_ARG;
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    free_all(c);
+    mps_config& f = c->cfg;
+    c->n = n;
+    c->pitch = (n + 31) / 32 * 32;
+    c->gp = c->wp = c->fp = 0;
+    for (int i = 0; i < n; i++) {
+        if (ptype[i] < 0) c->gp++;
+        else if (ptype[i] == 0) c->wp++;
+        else c->fp++;
+    }
+    if (!(f.xmin < f.xmax)) {
+        // grown bounding box and PMAX of main.cu:612-715, 548
+        double mn[3] = {99999999, 99999999, 99999999}, mx[3] = {-99999999, -99999999, -99999999};
+        for (int i = 0; i < n; i++) {
+            double q[3] = {x[i], y[i], f.dim == 3 ? z[i] : 0.0};
+            for (int a = 0; a < f.dim; a++) {
+                if (q[a] < mn[a]) mn[a] = q[a];
+                if (q[a] > mx[a]) mx[a] = q[a];
+            }
+        }
+        f.xmin = mn[0] - f.l0; f.xmax = mx[0] + f.l0;
+        f.ymin = mn[1] - f.l0; f.ymax = mx[1] + f.l0;
+        if (f.dim == 3) { f.zmin = mn[2] - f.l0; f.zmax = mx[2] + f.l0; }
+        else { f.zmin = 99999999; f.zmax = -99999999; }
+        f.pmax = (double)n * 4.50;
+    }
+    c->gl = make_grid(f, f.re_l);
+    c->gs = make_grid(f, f.re_s);
+    if ((long long)c->gl.tnc > (1LL << 30) || (long long)c->gs.tnc > (1LL << 30)) {
+        c->msg = "cell grid too large";
+        return MPS_ERR_ARG;
+    }
+    bool strict = f.dim == 2;
+    c->cut_l = sqrt_cut(strict ? f.re_l : f.re_l + f.delta, strict);
+    c->cut_s = sqrt_cut(strict ? f.re_s : f.re_s + f.delta, strict);
+    c->cap_l = f.list_cap_l > 0 ? f.list_cap_l : auto_cap(f, f.re_l);
+    c->cap_s = f.list_cap_s > 0 ? f.list_cap_s : auto_cap(f, f.re_s);
+    c->lambda_l = 0.0;  // main.cu:491-494 at the Laplacian radius
+    double re = f.re_l;
+    if (f.ktype == 1) c->lambda_l = 0.22143 * (re * re);
+    if (f.ktype == 2) c->lambda_l = 0.16832 * (re * re);
+    if (f.ktype == 5) c->lambda_l = 0.250 * (re * re);
+    if (f.ktype == 6) c->lambda_l = 0.14288 * (re * re);
+    TRY(allocate(c));
+    cudaStream_t st = c->stream;
+    auto up = [&](double* d, const double* h) -> cudaError_t {
+        if (!h) return cudaMemsetAsync(d, 0, sizeof(double) * n, st);
+        return cudaMemcpyAsync(d, h, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    };
+    VMPS_CUDA(c, up(c->x, x));
+    VMPS_CUDA(c, up(c->y, y));
+    VMPS_CUDA(c, up(c->z, f.dim == 3 ? z : nullptr));
+    VMPS_CUDA(c, up(c->u, u));
+    VMPS_CUDA(c, up(c->v, v));
+    VMPS_CUDA(c, up(c->w, f.dim == 3 ? w : nullptr));
+    VMPS_CUDA(c, up(c->p, p));
+    VMPS_CUDA(c, cudaMemcpyAsync(c->ptype, ptype, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+    k_iota<<<grid_blocks(n), kBlock, 0, st>>>(n, c->oid);
+    k_density<<<grid_blocks(n), kBlock, 0, st>>>(n, c->ptype, f.rho1, f.rho2, c->rho);
+    vmps_count_launch(2);
+    VMPS_CUDA(c, cudaStreamSynchronize(st));
+    c->initialized = false;
+    c->steps = 0;
+    c->host_err = 0;
+    return MPS_OK;
+}
+
+int mps_load_grd(mps_ctx* c, const char* path)
+{
+    if (!c || !path) return MPS_ERR_ARG;
+    std::ifstream in(path);
+    if (!in.is_open()) {
+        c->msg = std::string("cannot open ") + path;
+        return MPS_ERR_IO;
+    }
+    int n = 0;
+    in >> n;
+    if (n <= 0) return MPS_ERR_IO;
+    bool three = c->cfg.dim == 3;
+    std::vector<double> x(n), y(n), z(n), u(n), v(n), w(n), p(n);
+    std::vector<int> pt(n);
+    for (int i = 0; i < n; i++) {  // main.cu:629-661
+        in >> x[i] >> y[i];
+        if (three) in >> z[i];
+        in >> pt[i] >> u[i] >> v[i];
+        if (three) in >> w[i];
+        in >> p[i];
+        if (!in) {
+            c->msg = "truncated .grd file";
+            return MPS_ERR_IO;
+        }
+    }
+    return mps_upload(c, n, x.data(), y.data(), z.data(), pt.data(), u.data(), v.data(), w.data(),
+                      p.data());
+}
+
+int mps_neighbors(mps_ctx* c)
+{
+    if (!c || c->n == 0) return MPS_ERR_ARG;
+    return vmps_neighbors(c);
+}
+
+int mps_init(mps_ctx* c)
+{
+    if (!c || c->n == 0) return MPS_ERR_ARG;
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    TRY(vmps_neighbors(c));
+    VMPS_CUDA(c, cudaMemsetAsync(c->d_max, 0, sizeof(unsigned long long), c->stream));
+    TRY(vmps_pnd(c, 0, 1, 1, c->nd));
+    TRY(device_max(c, &c->n0_s));
+    if (c->cfg.re_s == c->cfg.re_l) {
+        c->n0_l = c->n0_s;
+    } else {
+        VMPS_CUDA(c, cudaMemsetAsync(c->d_max, 0, sizeof(unsigned long long), c->stream));
+        TRY(vmps_pnd(c, 0, 1, 0, c->nds));
+        TRY(device_max(c, &c->n0_l));
+    }
+    VMPS_CUDA(c, cudaMemcpyAsync(c->pnew, c->p, sizeof(double) * c->n, cudaMemcpyDeviceToDevice,
+                                 c->stream));
+    c->initialized = true;
+    int e = collect_errors(c);
+    return e;
+}
+
+#define NEED_INIT(c)                                   \
+    do {                                               \
+        if (!(c) || !(c)->initialized) return MPS_ERR_ARG; \
+    } while (0)
+
+int mps_pnd(mps_ctx* c) { NEED_INIT(c); return vmps_pnd(c, 0, 1, 1, c->nd); }
+int mps_sps(mps_ctx* c) { NEED_INIT(c); return vmps_sps(c); }
+int mps_vfraction(mps_ctx* c) { NEED_INIT(c); return vmps_vfraction(c); }
+int mps_viscosity(mps_ctx* c) { NEED_INIT(c); return vmps_viscosity(c); }
+int mps_predict(mps_ctx* c) { NEED_INIT(c); return vmps_predict(c); }
+int mps_pnd_star(mps_ctx* c) { NEED_INIT(c); return vmps_pnd(c, 1, 0, 1, c->nds); }
+int mps_bcon(mps_ctx* c) { NEED_INIT(c); return vmps_bcon(c); }
+int mps_phat(mps_ctx* c) { NEED_INIT(c); return vmps_phat(c); }
+int mps_pressure_gradient(mps_ctx* c) { NEED_INIT(c); return vmps_pressgrad(c); }
+int mps_integrate(mps_ctx* c) { NEED_INIT(c); return vmps_integrate(c); }
+int mps_collision(mps_ctx* c) { NEED_INIT(c); return vmps_collision(c); }
+int mps_commit(mps_ctx* c)
+{
+    NEED_INIT(c);
+    TRY(vmps_commit(c));
+    return collect_errors(c);
+}
+
+int mps_pressure(mps_ctx* c, int* iters, double* relres)
+{
+    NEED_INIT(c);
+    if (c->cfg.method == 3) {
+        TRY(vmps_pressure_wc(c));
+        c->cg_iters = 0;
+        c->cg_relres = 0;
+    } else {
+        TRY(vmps_ppe(c));
+    }
+    if (iters) *iters = c->cg_iters;
+    if (relres) *relres = c->cg_relres;
+    return MPS_OK;
+}
+
+int mps_step(mps_ctx* c)
+{
+    NEED_INIT(c);
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    const mps_config& f = c->cfg;
+    unsigned int before = c->host_err;
+    auto mark = [&](int k) -> int {
+        if (c->profile) VMPS_CUDA(c, cudaEventRecord(c->ev[k], c->stream));
+        return MPS_OK;
+    };
+    TRY(mark(0));
+    if (f.method != 3 && !f.ppe_at_predicted) TRY(vmps_pnd(c, 0, 1, 1, c->nd));
+    TRY(vmps_neighbors(c));
+    TRY(mark(1));
+    if (f.turb) TRY(vmps_sps(c));
+    TRY(vmps_vfraction(c));
+    TRY(vmps_viscosity(c));
+    TRY(vmps_predict(c));
+    TRY(vmps_pnd(c, 1, 0, 1, c->nds));
+    if (f.method != 3) TRY(vmps_bcon(c));
+    TRY(mark(2));
+    if (f.method != 3) TRY(vmps_ppe(c));
+    else TRY(vmps_pressure_wc(c));
+    TRY(mark(3));
+    TRY(vmps_phat(c));
+    TRY(vmps_pressgrad(c));
+    TRY(vmps_integrate(c));
+    TRY(vmps_collision(c));
+    TRY(vmps_commit(c));
+    TRY(mark(4));
+    c->steps++;
+    int e = collect_errors(c);
+    if (c->profile) {
+        for (int k = 0; k < 4; k++) {
+            float ms = 0;
+            VMPS_CUDA(c, cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]));
+            c->ms_stage[k] = ms;
+        }
+        float ms = 0;
+        VMPS_CUDA(c, cudaEventElapsedTime(&ms, c->ev[0], c->ev[4]));
+        c->ms_stage[4] = ms;
+    }
+    return e | (int)(c->host_err & ~before);
+}
+
+int mps_run(mps_ctx* c, int steps)
+{
+    int acc = 0;
+    for (int s = 0; s < steps; s++) {
+        int r = mps_step(c);
+        if (r & (MPS_ERR_ARG | MPS_ERR_CUDA)) return r;
+        acc |= r;
+    }
+    return acc;
+}
+
+int mps_set_state(mps_ctx* c, const double* x, const double* y, const double* z,
+                  const double* u, const double* v, const double* w, const double* p)
+{
+    NEED_INIT(c);
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    const int n = c->n;
+    const double* src[7] = {x, y, z, u, v, w, p};
+    double* dst[7] = {c->x, c->y, c->z, c->u, c->v, c->w, c->p};
+    for (int k = 0; k < 7; k++) {
+        if (!src[k] || (c->cfg.dim == 2 && (k == 2 || k == 5))) continue;
+        VMPS_CUDA(c, cudaMemcpyAsync(c->stage_in, src[k], sizeof(double) * n,
+                                     cudaMemcpyHostToDevice, c->stream));
+        k_permute_in<<<grid_blocks(n), kBlock, 0, c->stream>>>(n, c->oid, c->stage_in, dst[k],
+                                                               k == 6 ? c->pnew : nullptr);
+        vmps_count_launch(1);
+    }
+    VMPS_CUDA(c, cudaGetLastError());
+    return MPS_OK;
+}
+
+int mps_get_state(mps_ctx* c, double* x, double* y, double* z, double* u, double* v, double* w,
+                  double* p)
+{
+    NEED_INIT(c);
+    const char* names[7] = {"x", "y", "z", "u", "v", "w", "p"};
+    double* out[7] = {x, y, z, u, v, w, p};
+    for (int k = 0; k < 7; k++) {
+        if (!out[k] || (c->cfg.dim == 2 && (k == 2 || k == 5))) continue;
+        TRY(mps_download(c, names[k], out[k], nullptr));
+    }
+    return MPS_OK;
+}
+
+int mps_set_profile(mps_ctx* c, int on)
+{
+    if (!c) return MPS_ERR_ARG;
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    if (on && !c->ev[0])
+        for (auto& e : c->ev) VMPS_CUDA(c, cudaEventCreate(&e));
+    c->profile = on != 0;
+    c->spmv_ms = c->lists_ms = 0;
+    c->spmv_launches = c->lists_launches = 0;
+    return MPS_OK;
+}
+
+int mps_download(mps_ctx* c, const char* field, void* out, long* count)
+{
+    if (!c || !field || c->n == 0) return MPS_ERR_ARG;
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    const int n = c->n;
+    std::string f(field);
+    cudaStream_t st = c->stream;
+    if (count) *count = n;
+    if (!out) return MPS_OK;
+    // S6 column-0 area doubles as the staging buffer (6 * pitch doubles)
+    double* stage = c->S6;
+    int* istage = (int*)c->S6;
+    if (double* a = field_d(c, f)) {
+        k_unpermute_d<<<grid_blocks(n), kBlock, 0, st>>>(n, c->oid, a, stage);
+        VMPS_CUDA(c, cudaMemcpyAsync(out, stage, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    } else if (f == "ptype" || f == "bcon" || f == "cell_l" || f == "cell_s") {
+        const int* a = f == "ptype" ? c->ptype : f == "bcon" ? c->bcon : f == "cell_l" ? c->cell_l
+                                                                                       : c->cell_s;
+        k_unpermute_i<<<grid_blocks(n), kBlock, 0, st>>>(n, c->oid, a, istage);
+        VMPS_CUDA(c, cudaMemcpyAsync(out, istage, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+    } else if (f == "perm_l" || f == "perm_s") {
+        k_perm_ids<<<grid_blocks(n), kBlock, 0, st>>>(n, c->oid, f == "perm_s" ? c->perm_s : nullptr,
+                                                       istage);
+        VMPS_CUDA(c, cudaMemcpyAsync(out, istage, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+    } else {
+        c->msg = "unknown field " + f;
+        return MPS_ERR_ARG;
+    }
+    vmps_count_launch(1);
+    VMPS_CUDA(c, cudaStreamSynchronize(st));
+    return MPS_OK;
+}
+
+int mps_download_lists(mps_ctx* c, int which, int* off, int* nbr, long* total)
+{
+    if (!c || c->n == 0 || (which != 0 && which != 1)) return MPS_ERR_ARG;
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    const int n = c->n, P = c->pitch;
+    int cap = which == 0 ? c->cap_s : c->cap_l;
+    const int* dl = which == 0 ? c->len_s : c->len_l;
+    const int* dn = which == 0 ? c->nbr_s : c->nbr_l;
+    std::vector<int> len(n), oid(n), ent((size_t)cap * P);
+    VMPS_CUDA(c, cudaMemcpy(len.data(), dl, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    VMPS_CUDA(c, cudaMemcpy(oid.data(), c->oid, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    VMPS_CUDA(c, cudaMemcpy(ent.data(), dn, sizeof(int) * ent.size(), cudaMemcpyDeviceToHost));
+    std::vector<int> slot_of(n);
+    for (int i = 0; i < n; i++) slot_of[oid[i]] = i;
+    long tot = 0;
+    for (int q = 0; q < n; q++) tot += len[slot_of[q]];
+    if (total) *total = tot;
+    if (!off) return MPS_OK;
+    long acc = 0;
+    for (int q = 0; q < n; q++) {
+        int i = slot_of[q];
+        off[q] = (int)acc;
+        if (nbr)
+            for (int k = 0; k < len[i]; k++) nbr[acc + k] = oid[ent[(size_t)k * P + i]];
+        acc += len[i];
+    }
+    off[n] = (int)acc;
+    return MPS_OK;
+}
+
+int mps_get_scalar(mps_ctx* c, const char* name, double* out)
+{
+    if (!c || !name || !out) return MPS_ERR_ARG;
+    std::string s(name);
+    if (s == "n0_s") *out = c->n0_s;
+    else if (s == "n0_l") *out = c->n0_l;
+    else if (s == "lambda_l") *out = c->lambda_l;
+    else if (s == "cg_iters") *out = c->cg_iters;
+    else if (s == "cg_relres") *out = c->cg_relres;
+    else if (s == "n") *out = c->n;
+    else if (s == "steps") *out = (double)c->steps;
+    else if (s == "cap_s") *out = c->cap_s;
+    else if (s == "cap_l") *out = c->cap_l;
+    else if (s == "launches") *out = (double)g_launches.load();
+    else if (s == "ms_neighbors") *out = c->ms_stage[0];
+    else if (s == "ms_explicit") *out = c->ms_stage[1];
+    else if (s == "ms_ppe") *out = c->ms_stage[2];
+    else if (s == "ms_post") *out = c->ms_stage[3];
+    else if (s == "ms_step") *out = c->ms_stage[4];
+    else if (s == "spmv_ms") *out = c->spmv_ms;
+    else if (s == "spmv_launches") *out = (double)c->spmv_launches;
+    else if (s == "lists_ms") *out = c->lists_ms;
+    else if (s == "lists_launches") *out = (double)c->lists_launches;
+    else if (s == "pmax") *out = c->cfg.pmax;
+    else if (s == "xmin") *out = c->cfg.xmin;
+    else if (s == "xmax") *out = c->cfg.xmax;
+    else if (s == "ymin") *out = c->cfg.ymin;
+    else if (s == "ymax") *out = c->cfg.ymax;
+    else if (s == "zmin") *out = c->cfg.zmin;
+    else if (s == "zmax") *out = c->cfg.zmax;
+    else if (s == "len_max_l" || s == "len_max_s") {
+        int h[2] = {0, 0};
+        VMPS_CUDA(c, cudaMemcpy(h, c->len_max, sizeof(h), cudaMemcpyDeviceToHost));
+        *out = s == "len_max_l" ? h[0] : h[1];
+    } else if (s == "nnz_l" || s == "nnz_s" || s == "nnz_a") {
+        std::vector<int> len(c->n);
+        const int* d = s == "nnz_l" ? c->len_l : s == "nnz_s" ? c->len_s : c->mlen;
+        VMPS_CUDA(c, cudaMemcpy(len.data(), d, sizeof(int) * c->n, cudaMemcpyDeviceToHost));
+        double t = 0;
+        for (int v : len) t += v;
+        *out = t;
+    } else {
+        return MPS_ERR_ARG;
+    }
+    return MPS_OK;
+}
+
+int mps_get_error(mps_ctx* c)
+{
+    if (!c) return MPS_ERR_ARG;
+    int e = (int)c->host_err;
+    c->host_err = 0;
+    return e;
+}
+
+const char* mps_last_message(mps_ctx* c) { return c ? c->msg.c_str() : ""; }
+
+void* mps_stream(mps_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int mps_write_vtu(mps_ctx* c, const char* path, int fluid_only)
+{
+    if (!c || !path || c->n == 0) return MPS_ERR_ARG;
+    const int n = c->n;
+    std::vector<double> x(n), y(n), z(n), u(n), v(n), w(n), p(n);
+    std::vector<int> pt(n);
+    const char* names[] = {"x", "y", "z", "u", "v", "w", "p"};
+    double* dst[] = {x.data(), y.data(), z.data(), u.data(), v.data(), w.data(), p.data()};
+    for (int k = 0; k < 7; k++) TRY(mps_download(c, names[k], dst[k], nullptr));
+    TRY(mps_download(c, "ptype", pt.data(), nullptr));
+    std::vector<int> keep;
+    for (int i = 0; i < n; i++)
+        if (!fluid_only || pt[i] > 0) keep.push_back(i);
+    FILE* fp = fopen(path, "w");
+    if (!fp) return MPS_ERR_IO;
+    // inOut.cpp:122-216 layout; all three components are written in 3D (the
+    // reference drops z and w there, inOut.cpp:135,154)
+    int m = (int)keep.size();
+    bool three = c->cfg.dim == 3;
+    fprintf(fp, "<?xml version='1.0' encoding='UTF-8'?>\n");
+    fprintf(fp, "<VTKFile xmlns='VTK' byte_order='LittleEndian' version='0.1' type='UnstructuredGrid'>\n");
+    fprintf(fp, " <UnstructuredGrid>\n  <Piece NumberOfCells='%d' NumberOfPoints='%d'>\n", m, m);
+    fprintf(fp, "   <Points>\n    <DataArray NumberOfComponents='3' type='Float32' Name='Position' format='ascii'>\n");
+    for (int i : keep) fprintf(fp, "%.9g %.9g %.9g ", x[i], y[i], three ? z[i] : 0.0);
+    fprintf(fp, "\n    </DataArray>\n   </Points>\n   <PointData>\n");
+    fprintf(fp, "    <DataArray NumberOfComponents='3' type='Float32' Name='Velocity' format='ascii'>\n");
+    for (int i : keep) fprintf(fp, "%.9g %.9g %.9g ", u[i], v[i], three ? w[i] : 0.0);
+    fprintf(fp, "\n    </DataArray>\n    <DataArray NumberOfComponents='1' type='Float32' Name='Pressure' format='ascii'>\n");
+    for (int i : keep) fprintf(fp, "%.9g ", p[i]);
+    fprintf(fp, "\n    </DataArray>\n    <DataArray NumberOfComponents='1' type='Int32' Name='partType' format='ascii'>\n");
+    for (int i : keep) fprintf(fp, "%d ", pt[i]);
+    fprintf(fp, "\n    </DataArray>\n   </PointData>\n   <Cells>\n    <DataArray type='Int32' Name='connectivity' format='ascii'>\n");
+    for (int b = 0; b < m; b++) fprintf(fp, "%d ", b);
+    fprintf(fp, "\n    </DataArray>\n    <DataArray type='Int32' Name='offsets' format='ascii'>\n");
+    for (int b = 1; b <= m; b++) fprintf(fp, "%d ", b);
+    fprintf(fp, "\n    </DataArray>\n    <DataArray type='UInt8' Name='types' format='ascii'>\n");
+    for (int b = 0; b < m; b++) fprintf(fp, "1 ");
+    fprintf(fp, "\n    </DataArray>\n   </Cells>\n  </Piece>\n </UnstructuredGrid>\n</VTKFile>");
+    int bad = ferror(fp);
+    fclose(fp);
+    return bad ? MPS_ERR_IO : MPS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,220 @@
+// mps_internal.cuh -- context layout and device helpers shared by the
+// solver's translation units.
+//
+// Layout in HBM: structure-of-arrays, particles in cell order (re-sorted
+// every step by (cell, original id), the order NEIGHBOR's counting sort
+// produces, functions.cu:2820-2852).  Neighbour lists and the PPE matrix are
+// slot-major ELL: entry k of row i lives at k * pitch + i, so a warp of 32
+// consecutive rows reads 128 contiguous bytes per slot.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/voxarmps.h"
+
+namespace vmps {
+
+constexpr int kBlock = 256;
+
+// Cell grid of one support radius, NEIGHBOR's (functions.cu:2790-2802): x and
+// y cells of size re, z cells of size re + DELTA (3D).
+struct Grid {
+    int ncx, ncy, ncz, tnc;
+    double re, rez;
+    double xmin, ymin, zmin;
+};
+
+// Squared-distance thresholds equivalent to the reference's sqrt() compares
+// (sqrt is correctly rounded on host and device, so the equivalence is exact).
+struct Cutoff {
+    double d2;       // 2D: d2 < d2 (strict); 3D: d2 <= d2
+    int dim;
+};
+
+struct DeviceError {
+    unsigned int bits;
+};
+
+}  // namespace vmps
+
+struct mps_ctx {
+    mps_config cfg;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string msg;
+    int n = 0, pitch = 0;
+    int gp = 0, wp = 0, fp = 0;
+    vmps::Grid gl{}, gs{};
+    double cut_l = 0, cut_s = 0;  // squared-distance thresholds
+    int cap_l = 0, cap_s = 0;
+    double n0_s = 0, n0_l = 0, lambda_l = 0;
+    int cg_iters = 0;
+    double cg_relres = 0;
+    long steps = 0;
+    bool initialized = false;
+    unsigned int host_err = 0;
+
+    // persistent particle state, cell order (double-buffered for the reorder)
+    double *x = nullptr, *y = nullptr, *z = nullptr, *u = nullptr, *v = nullptr, *w = nullptr;
+    double *p = nullptr, *pnew = nullptr, *phat = nullptr, *un = nullptr, *vn = nullptr,
+           *wn = nullptr, *rho = nullptr, *nd = nullptr;
+    int *ptype = nullptr, *oid = nullptr;
+    // per-step scratch fields
+    double *xs = nullptr, *ys = nullptr, *zs = nullptr, *us = nullptr, *vs = nullptr,
+           *ws = nullptr, *nds = nullptr, *C = nullptr, *meu = nullptr, *neut = nullptr,
+           *t1 = nullptr, *t2 = nullptr, *t3 = nullptr, *source = nullptr, *diag = nullptr;
+    int* bcon = nullptr;
+    // SPS strain tensor (6 comps) and collision outputs (swapped with the state)
+    double* S6 = nullptr;
+    double *xc = nullptr, *yc = nullptr, *zc = nullptr, *uc = nullptr, *vc = nullptr,
+           *wc = nullptr;
+    // sort / cells
+    int *cell_l = nullptr, *cell_s = nullptr;      // per slot, 1-based Cnum
+    int *bpos_l = nullptr, *bpos_s = nullptr;      // position inside the bucket
+    int *cnt_l = nullptr, *cst_l = nullptr;        // per cell count / start
+    int *cnt_s = nullptr, *cst_s = nullptr;
+    int *bslot_l = nullptr, *boid_l = nullptr;     // bucketed slots / ids
+    int *bslot_s = nullptr, *boid_s = nullptr;
+    int *src = nullptr, *inv = nullptr;            // new slot <- old slot, old -> new
+    int *perm_s = nullptr, *perm_s_tmp = nullptr;  // small-grid cell order (slots)
+    // lists (slot-major)
+    int *nbr_l = nullptr, *len_l = nullptr, *nbr_s = nullptr, *len_s = nullptr;
+    // PPE matrix (compact slot-major ELL) and CG vectors
+    int *mcol = nullptr, *mlen = nullptr;
+    double* mval = nullptr;
+    double *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_s = nullptr;
+    double* cg_part = nullptr;   // block partial sums
+    double* cg_scal = nullptr;   // device scalars (rz, bb, rr, ...)
+    int* cg_flag = nullptr;      // [0] done, [1] iterations
+    int* cg_flag_host = nullptr; // pinned
+    double* red_host = nullptr;  // pinned scratch for scalars
+    unsigned int* d_err = nullptr;
+    unsigned int* h_err = nullptr;  // pinned
+    int* len_max = nullptr;         // [0] max len_l, [1] max len_s (diagnostics)
+    unsigned long long* d_max = nullptr;  // atomic max of a non-negative double
+    int* scan_tmp = nullptr;        // tile sums of the cell-count scans
+    double* stage_in = nullptr;     // H2D staging for mps_set_state
+    // profiling (CUDA events on the context stream)
+    bool profile = false;
+    cudaEvent_t ev[8] = {};
+    std::vector<cudaEvent_t> ev_spmv;
+    double ms_stage[5] = {0, 0, 0, 0, 0};
+    double spmv_ms = 0, lists_ms = 0;
+    long spmv_launches = 0, lists_launches = 0;
+    // reorder double-buffers (same shapes as the persistent fields)
+    std::vector<void*> alts;
+    std::vector<void*> owned;
+    std::vector<void*> pinned;
+};
+
+namespace vmps {
+
+// ---------------- device helpers (exact IEEE FP64, no contraction) ----------
+// Every FP64 translation unit is compiled with -fmad=false so that a*b + c is
+// two roundings, as in the reference's x86 build.
+
+__host__ __device__ inline double kernel_w(double R, int ktype, int dim, double re)
+{
+    // W(), functions.cu:32-74
+    double w = 0.0;
+    double q = R / re;
+    switch (ktype) {
+    case 1:
+        if (q < 0.5) w = 2.0 - 4.0 * (q * q);
+        else if (q <= 1.0) w = (2 * q - 2) * (2 * q - 2);
+        else w = 0;
+        break;
+    case 2:
+        if (q < 1.0) w = (1 / q) - 1;
+        else w = 0;
+        break;
+    case 3: {
+        double Cc = 0.0;
+        if (dim == 1) Cc = 0.6666;
+        if (dim == 2) Cc = 1.43 * 3.14;
+        if (dim == 3) Cc = 1 / 3.14;
+        if (R < re) w = Cc / pow(re, (double)dim) * (1 - 1.5 * (q * q) + 0.75 * pow(q, 3.0));
+        else if (R >= re && R < (2.0 * re)) w = Cc / pow(re, (double)dim) * (0.25 * pow(2.0 - q, 3.0));
+        else w = 0;
+        break;
+    }
+    case 5:
+        if (q <= 1.0) w = 1.5 * log(1 / (q + 0.000001));
+        else w = 0;
+        break;
+    case 6:
+        if (q <= 1.0) w = pow((1 - q), 3.0);
+        else w = 0;
+        break;
+    }
+    return w;
+}
+
+template <int DIM>
+__device__ __forceinline__ double dist2(double dx, double dy, double dz)
+{
+    // pow(dx,2)+pow(dy,2)[+pow(dz,2)] as the reference's -O2 build evaluates it
+    if (DIM == 3) return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+    return __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+}
+
+__device__ __forceinline__ void set_error(unsigned int* e, unsigned int bit)
+{
+    atomicOr(e, bit);
+}
+
+// Cell of a position in one grid (functions.cu:2823-2835); returns false when
+// the reference's int() would leave [1, nc] on some axis.
+template <int DIM>
+__device__ __forceinline__ bool cell_coords(const Grid& g, double x, double y, double z, int& ic,
+                                            int& jc, int& kc)
+{
+    double fx = __ddiv_rn(x - g.xmin, g.re);
+    double fy = __ddiv_rn(y - g.ymin, g.re);
+    bool ok = (fx > -1.0) && (fx < (double)g.ncx) && (fy > -1.0) && (fy < (double)g.ncy);
+    ic = ok ? (int)fx + 1 : 1;
+    jc = ok ? (int)fy + 1 : 1;
+    kc = 1;
+    if (DIM == 3) {
+        double fz = __ddiv_rn(z - g.zmin, g.rez);
+        bool okz = (fz > -1.0) && (fz < (double)g.ncz);
+        kc = okz ? (int)fz + 1 : 1;
+        ok = ok && okz;
+    }
+    return ok;
+}
+
+inline int grid_blocks(long n) { return (int)((n + kBlock - 1) / kBlock); }
+
+}  // namespace vmps
+
+// host-side helpers implemented in mps_context.cu
+int vmps_check(mps_ctx* ctx, cudaError_t e, const char* what);
+#define VMPS_CUDA(ctx, call)                                   \
+    do {                                                       \
+        cudaError_t _e = (call);                               \
+        if (_e != cudaSuccess) return vmps_check(ctx, _e, #call); \
+    } while (0)
+
+// stage launchers (defined in the kernel translation units)
+int vmps_neighbors(mps_ctx* ctx);
+int vmps_pnd(mps_ctx* ctx, int at_star, int correct, int which_list, double* out);
+int vmps_max_reduce(mps_ctx* ctx, const double* a, double* result);
+int vmps_sps(mps_ctx* ctx);
+int vmps_vfraction(mps_ctx* ctx);
+int vmps_viscosity(mps_ctx* ctx);
+int vmps_predict(mps_ctx* ctx);
+int vmps_bcon(mps_ctx* ctx);
+int vmps_pressure_wc(mps_ctx* ctx);
+int vmps_ppe(mps_ctx* ctx);
+int vmps_phat(mps_ctx* ctx);
+int vmps_pressgrad(mps_ctx* ctx);
+int vmps_integrate(mps_ctx* ctx);
+int vmps_collision(mps_ctx* ctx);
+int vmps_commit(mps_ctx* ctx);
+int vmps_count_launch(int k);

@@ -1,0 +1,357 @@
+// mps_neighbors.cu -- hash, sort, reorder and neighbour lists (NEIGHBOR,
+// functions.cu:2788-2929; the reference GPU path's calcHash / sort_by_key /
+// findCellStart / createNeighbourArrays, neighbour_parallel.cu:37-199).
+//
+// Per step:
+//   1. k_hash      exact FP64 cell number of every particle on both grids
+//                  (Laplacian grid = primary order, PND grid = index only),
+//                  bucket counts by atomics;
+//   2. scan        exclusive prefix sums of the counts (cell starts);
+//   3. k_scatter   particles into their cell bucket (arbitrary order);
+//   4. k_rank      order inside a bucket by original id: the stable counting
+//                  sort of the reference's insertion loop (functions.cu:2820);
+//   5. k_gather    reorder the persistent particle state into cell order;
+//   6. k_lists     both lists in the reference's scan order (row, colu, dep;
+//                  ascending id inside a cell), membership decided with the
+//                  reference's exact FP64 arithmetic.
+#include <cstdio>
+
+#include "mps_internal.cuh"
+
+using namespace vmps;
+
+namespace {
+
+template <int DIM>
+__global__ void k_hash(int n, Grid gl, Grid gs, const double* __restrict__ x,
+                       const double* __restrict__ y, const double* __restrict__ z,
+                       int* __restrict__ cell_l, int* __restrict__ cell_s,
+                       int* __restrict__ cnt_l, int* __restrict__ cnt_s,
+                       int* __restrict__ bpos_l, int* __restrict__ bpos_s, unsigned int* err)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double xi = x[i], yi = y[i], zi = DIM == 3 ? z[i] : 0.0;
+    int a, b, c;
+    bool ok = cell_coords<DIM>(gl, xi, yi, zi, a, b, c);
+    int Cl = a + (b - 1) * gl.ncx + (c - 1) * gl.ncx * gl.ncy;
+    ok = cell_coords<DIM>(gs, xi, yi, zi, a, b, c) && ok;
+    int Cs = a + (b - 1) * gs.ncx + (c - 1) * gs.ncx * gs.ncy;
+    if (!ok) set_error(err, MPS_ERR_CELL);
+    cell_l[i] = Cl;
+    cell_s[i] = Cs;
+    bpos_l[i] = atomicAdd(&cnt_l[Cl], 1);
+    bpos_s[i] = atomicAdd(&cnt_s[Cs], 1);
+}
+
+// three-phase exclusive scan (tile sums, scan of tile sums, tile rescans)
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* sh, int* total)
+{
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) sh[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        int s = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0;
+        int si = s;
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, si, o);
+            if (lane >= o) si += t;
+        }
+        sh[lane] = si - s;
+        if (lane == 31) sh[32] = si;
+    }
+    __syncthreads();
+    int r = inc - v + sh[wid];
+    if (total) *total = sh[32];
+    __syncthreads();
+    return r;
+}
+
+__global__ void k_scan_tiles(int m, const int* __restrict__ in, int* __restrict__ tile_sum)
+{
+    __shared__ int sh[33];
+    int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    int s = 0;
+    for (int k = 0; k < kScanItems; k++)
+        if (base + k < m) s += in[base + k];
+    int tot;
+    block_exclusive_scan(s, sh, &tot);
+    if (threadIdx.x == 0) tile_sum[blockIdx.x] = tot;
+}
+
+__global__ void k_scan_sums(int tiles, int* tile_sum)
+{
+    __shared__ int sh[33];
+    int carry = 0;
+    for (int base = 0; base < tiles; base += kScanThreads) {
+        int i = base + threadIdx.x;
+        int v = i < tiles ? tile_sum[i] : 0;
+        int tot;
+        int e = block_exclusive_scan(v, sh, &tot);
+        if (i < tiles) tile_sum[i] = e + carry;
+        carry += tot;
+        __syncthreads();
+    }
+}
+
+__global__ void k_scan_apply(int m, const int* __restrict__ in, const int* __restrict__ tile_sum,
+                             int* __restrict__ out)
+{
+    __shared__ int sh[33];
+    int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    int vals[kScanItems];
+    int s = 0;
+    for (int k = 0; k < kScanItems; k++) {
+        vals[k] = (base + k < m) ? in[base + k] : 0;
+        s += vals[k];
+    }
+    int e = block_exclusive_scan(s, sh, nullptr) + tile_sum[blockIdx.x];
+    for (int k = 0; k < kScanItems; k++) {
+        if (base + k < m) out[base + k] = e;
+        e += vals[k];
+    }
+}
+
+__global__ void k_scatter(int n, const int* __restrict__ cell_l, const int* __restrict__ cell_s,
+                          const int* __restrict__ bpos_l, const int* __restrict__ bpos_s,
+                          const int* __restrict__ cst_l, const int* __restrict__ cst_s,
+                          const int* __restrict__ oid, int* __restrict__ bslot_l,
+                          int* __restrict__ boid_l, int* __restrict__ bslot_s,
+                          int* __restrict__ boid_s)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int o = oid[i];
+    int q = cst_l[cell_l[i]] + bpos_l[i];
+    bslot_l[q] = i;
+    boid_l[q] = o;
+    int qs = cst_s[cell_s[i]] + bpos_s[i];
+    bslot_s[qs] = i;
+    boid_s[qs] = o;
+}
+
+// Rank inside the bucket by original id.  Primary grid: src[new] = old slot
+// and inv[old] = new.  PND grid: perm_tmp[position] = old slot.
+__global__ void k_rank(int n, const int* __restrict__ cell_l, const int* __restrict__ cell_s,
+                       const int* __restrict__ cst_l, const int* __restrict__ cnt_l,
+                       const int* __restrict__ cst_s, const int* __restrict__ cnt_s,
+                       const int* __restrict__ bslot_l, const int* __restrict__ boid_l,
+                       const int* __restrict__ bslot_s, const int* __restrict__ boid_s,
+                       int* __restrict__ src, int* __restrict__ inv, int* __restrict__ perm_tmp)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    {
+        int s = bslot_l[q], me = boid_l[q];
+        int c = cell_l[s];
+        int b = cst_l[c], e = b + cnt_l[c], r = 0;
+        for (int t = b; t < e; t++) r += (boid_l[t] < me);
+        src[b + r] = s;
+        inv[s] = b + r;
+    }
+    {
+        int s = bslot_s[q], me = boid_s[q];
+        int c = cell_s[s];
+        int b = cst_s[c], e = b + cnt_s[c], r = 0;
+        for (int t = b; t < e; t++) r += (boid_s[t] < me);
+        perm_tmp[b + r] = s;
+    }
+}
+
+struct GatherSet {
+    const void* from[24];
+    void* to[24];
+    int elem[24];
+    int count;
+};
+
+__global__ void k_gather(int n, const int* __restrict__ src, GatherSet g)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int s = src[k];
+    for (int a = 0; a < g.count; a++) {
+        if (g.elem[a] == 8)
+            ((double*)g.to[a])[k] = ((const double*)g.from[a])[s];
+        else
+            ((int*)g.to[a])[k] = ((const int*)g.from[a])[s];
+    }
+}
+
+__global__ void k_translate(int n, const int* __restrict__ inv, const int* __restrict__ in,
+                            int* __restrict__ out)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) out[k] = inv[in[k]];
+}
+
+// Both lists, one thread per particle (reference scan order; see file head).
+template <int DIM>
+__global__ void k_lists(int n, int pitch, Grid gl, Grid gs, double cut_l, double cut_s,
+                        int cap_l, int cap_s, const double* __restrict__ x,
+                        const double* __restrict__ y, const double* __restrict__ z,
+                        const int* __restrict__ cell_l, const int* __restrict__ cell_s,
+                        const int* __restrict__ cst_l, const int* __restrict__ cnt_l,
+                        const int* __restrict__ cst_s, const int* __restrict__ cnt_s,
+                        const int* __restrict__ perm_s, int* __restrict__ nbr_l,
+                        int* __restrict__ len_l, int* __restrict__ nbr_s, int* __restrict__ len_s,
+                        int* len_max, unsigned int* err)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double xi = x[i], yi = y[i], zi = DIM == 3 ? z[i] : 0.0;
+    for (int pass = 0; pass < 2; pass++) {
+        const Grid& g = pass == 0 ? gl : gs;
+        int C = (pass == 0 ? cell_l[i] : cell_s[i]) - 1;
+        int ic = C % g.ncx + 1, jc = (C / g.ncx) % g.ncy + 1, kc = C / (g.ncx * g.ncy) + 1;
+        int m1 = (ic == 1) ? 0 : -1, m2 = (ic == g.ncx) ? 0 : 1;
+        int m3 = (jc == 1) ? 0 : -1, m4 = (jc == g.ncy) ? 0 : 1;
+        int m5 = 0, m6 = 0;
+        if (DIM == 3) { m5 = (kc == 1) ? 0 : -1; m6 = (kc == g.ncz) ? 0 : 1; }
+        const int* cst = pass == 0 ? cst_l : cst_s;
+        const int* cnt = pass == 0 ? cnt_l : cnt_s;
+        int* out = pass == 0 ? nbr_l : nbr_s;
+        int cap = pass == 0 ? cap_l : cap_s;
+        double cut = pass == 0 ? cut_l : cut_s;
+        int k = 0;
+        for (int row = m1; row <= m2; row++)
+            for (int colu = m3; colu <= m4; colu++)
+                for (int dep = m5; dep <= m6; dep++) {
+                    int Cn = ic + row + (jc - 1 + colu) * g.ncx + (kc - 1 + dep) * g.ncx * g.ncy;
+                    int b = cst[Cn], e = b + cnt[Cn];
+                    for (int jj = b; jj < e; jj++) {
+                        int j = pass == 0 ? jj : perm_s[jj];
+                        double d2 = dist2<DIM>(x[j] - xi, y[j] - yi, DIM == 3 ? z[j] - zi : 0.0);
+                        bool in = (DIM == 3) ? (d2 <= cut) : (j != i && d2 < cut);
+                        if (in) {
+                            if (k < cap) out[(size_t)k * pitch + i] = j;
+                            k++;
+                        }
+                    }
+                }
+        if (k > cap) {
+            set_error(err, MPS_ERR_LIST_OVERFLOW);
+            k = cap;
+        }
+        (pass == 0 ? len_l : len_s)[i] = k;
+        atomicMax(&len_max[pass], k);
+    }
+}
+
+int scan(mps_ctx* ctx, int m, const int* in, int* out, int* tile_sum)
+{
+    int tiles = (m + kScanTile - 1) / kScanTile;
+    k_scan_tiles<<<tiles, kScanThreads, 0, ctx->stream>>>(m, in, tile_sum);
+    k_scan_sums<<<1, kScanThreads, 0, ctx->stream>>>(tiles, tile_sum);
+    k_scan_apply<<<tiles, kScanThreads, 0, ctx->stream>>>(m, in, tile_sum, out);
+    vmps_count_launch(3);
+    return MPS_OK;
+}
+
+}  // namespace
+
+// Persistent fields carried through the reorder (all other fields are
+// recomputed each step before use).
+static void persistent_set(mps_ctx* ctx, GatherSet& g, std::vector<void**>& slots,
+                           std::vector<void*>& alts)
+{
+    g.count = 0;
+    slots.clear();
+    double** d[] = {&ctx->x, &ctx->y, &ctx->z, &ctx->u, &ctx->v, &ctx->w, &ctx->p, &ctx->pnew,
+                    &ctx->phat, &ctx->un, &ctx->vn, &ctx->wn, &ctx->rho, &ctx->nd};
+    int** ii[] = {&ctx->ptype, &ctx->oid, &ctx->cell_l, &ctx->cell_s};
+    for (auto f : d) {
+        g.from[g.count] = *f;
+        g.elem[g.count] = 8;
+        slots.push_back((void**)f);
+        g.count++;
+    }
+    for (auto f : ii) {
+        g.from[g.count] = *f;
+        g.elem[g.count] = 4;
+        slots.push_back((void**)f);
+        g.count++;
+    }
+    for (int a = 0; a < g.count; a++) g.to[a] = alts[a];
+}
+
+// Alternate buffers for the reorder live in ctx->owned after the primaries;
+// they are registered by vmps_alloc_reorder() in mps_context.cu.
+extern std::vector<void*>& vmps_reorder_alts(mps_ctx* ctx);
+
+int vmps_neighbors(mps_ctx* ctx)
+{
+    const int n = ctx->n;
+    cudaStream_t st = ctx->stream;
+    int nb = grid_blocks(n);
+    VMPS_CUDA(ctx, cudaMemsetAsync(ctx->cnt_l, 0, sizeof(int) * (ctx->gl.tnc + 2), st));
+    VMPS_CUDA(ctx, cudaMemsetAsync(ctx->cnt_s, 0, sizeof(int) * (ctx->gs.tnc + 2), st));
+    VMPS_CUDA(ctx, cudaMemsetAsync(ctx->len_max, 0, sizeof(int) * 2, st));
+    if (ctx->cfg.dim == 3)
+        k_hash<3><<<nb, kBlock, 0, st>>>(n, ctx->gl, ctx->gs, ctx->x, ctx->y, ctx->z, ctx->cell_l,
+                                         ctx->cell_s, ctx->cnt_l, ctx->cnt_s, ctx->bpos_l,
+                                         ctx->bpos_s, ctx->d_err);
+    else
+        k_hash<2><<<nb, kBlock, 0, st>>>(n, ctx->gl, ctx->gs, ctx->x, ctx->y, ctx->z, ctx->cell_l,
+                                         ctx->cell_s, ctx->cnt_l, ctx->cnt_s, ctx->bpos_l,
+                                         ctx->bpos_s, ctx->d_err);
+    vmps_count_launch(1);
+    scan(ctx, ctx->gl.tnc + 2, ctx->cnt_l, ctx->cst_l, ctx->scan_tmp);
+    scan(ctx, ctx->gs.tnc + 2, ctx->cnt_s, ctx->cst_s, ctx->scan_tmp);
+    k_scatter<<<nb, kBlock, 0, st>>>(n, ctx->cell_l, ctx->cell_s, ctx->bpos_l, ctx->bpos_s,
+                                     ctx->cst_l, ctx->cst_s, ctx->oid, ctx->bslot_l, ctx->boid_l,
+                                     ctx->bslot_s, ctx->boid_s);
+    k_rank<<<nb, kBlock, 0, st>>>(n, ctx->cell_l, ctx->cell_s, ctx->cst_l, ctx->cnt_l, ctx->cst_s,
+                                  ctx->cnt_s, ctx->bslot_l, ctx->boid_l, ctx->bslot_s,
+                                  ctx->boid_s, ctx->src, ctx->inv, ctx->perm_s_tmp);
+    vmps_count_launch(2);
+    // reorder persistent state into cell order
+    GatherSet g;
+    std::vector<void**> slots;
+    std::vector<void*>& alts = vmps_reorder_alts(ctx);
+    persistent_set(ctx, g, slots, alts);
+    k_gather<<<nb, kBlock, 0, st>>>(n, ctx->src, g);
+    vmps_count_launch(1);
+    for (int a = 0; a < g.count; a++) {
+        void* old = *slots[a];
+        *slots[a] = alts[a];
+        alts[a] = old;
+    }
+    k_translate<<<nb, kBlock, 0, st>>>(n, ctx->inv, ctx->perm_s_tmp, ctx->perm_s);
+    vmps_count_launch(1);
+    if (ctx->profile) VMPS_CUDA(ctx, cudaEventRecord(ctx->ev[6], st));
+    if (ctx->cfg.dim == 3)
+        k_lists<3><<<nb, kBlock, 0, st>>>(n, ctx->pitch, ctx->gl, ctx->gs, ctx->cut_l, ctx->cut_s,
+                                          ctx->cap_l, ctx->cap_s, ctx->x, ctx->y, ctx->z,
+                                          ctx->cell_l, ctx->cell_s, ctx->cst_l, ctx->cnt_l,
+                                          ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_l,
+                                          ctx->len_l, ctx->nbr_s, ctx->len_s, ctx->len_max,
+                                          ctx->d_err);
+    else
+        k_lists<2><<<nb, kBlock, 0, st>>>(n, ctx->pitch, ctx->gl, ctx->gs, ctx->cut_l, ctx->cut_s,
+                                          ctx->cap_l, ctx->cap_s, ctx->x, ctx->y, ctx->z,
+                                          ctx->cell_l, ctx->cell_s, ctx->cst_l, ctx->cnt_l,
+                                          ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_l,
+                                          ctx->len_l, ctx->nbr_s, ctx->len_s, ctx->len_max,
+                                          ctx->d_err);
+    vmps_count_launch(1);
+    if (ctx->profile) {
+        VMPS_CUDA(ctx, cudaEventRecord(ctx->ev[7], st));
+        VMPS_CUDA(ctx, cudaEventSynchronize(ctx->ev[7]));
+        float ms = 0;
+        VMPS_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev[6], ctx->ev[7]));
+        ctx->lists_ms += ms;
+        ctx->lists_launches++;
+    }
+    VMPS_CUDA(ctx, cudaGetLastError());
+    return MPS_OK;
+}

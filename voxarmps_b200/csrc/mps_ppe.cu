@@ -1,0 +1,429 @@
+// mps_ppe.cu -- pressure Poisson equation: assembly and CG (PRESSURECALC
+// Method 1, functions.cu:2465-2549; MATRIX functions.cu:869-1005; CGM
+// functions.cu:506-716).
+//
+// Assembly keeps the reference's coefficients and diagonal (including the
+// 1e-7/dt^2 compressibility term) but stores only the columns that can be
+// non-zero in A*x: unknown (bcon == 0) neighbours with a non-zero weight.
+// Dirichlet columns (bcon == 1, p fixed at 0) add to the diagonal only.
+//
+// The solver is Jacobi-preconditioned (or plain) CG on the unknown rows,
+// stopped on the relative residual ||r||/||b|| <= cg_tol.  Dot products
+// reduce in FP64 through fixed per-block partials that every consumer block
+// re-reduces in the same order: deterministic, no atomics, no host sync per
+// iteration.  A device flag ends the iteration; the host checks it every few
+// iterations.
+#include "mps_internal.cuh"
+
+using namespace vmps;
+
+namespace {
+
+enum { S_BB = 0, S_RZ, S_RR, S_ZERO, S_NEWRZ, S_NEWRR, S_DONE, S_COUNT };
+constexpr int kRedThreads = 256;
+
+__device__ __forceinline__ double block_sum(double v, double* sh)
+{
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) r += sh[k];
+        sh[32] = r;
+    }
+    __syncthreads();
+    r = sh[32];
+    __syncthreads();
+    return r;
+}
+
+// every block reduces the same partials in the same order
+__device__ __forceinline__ double reduce_parts(const double* part, int nparts, double* sh)
+{
+    double v = 0.0;
+    for (int k = threadIdx.x; k < nparts; k += blockDim.x) v += part[k];
+    return block_sum(v, sh);
+}
+
+struct Asm {
+    double re, lambda, n0_l, n0_s, rho, dt;
+    int ktype, matopt, srcopt;
+};
+
+template <int DIM>
+__global__ void k_assemble(int n, int pitch, Asm A, const int* __restrict__ nbr,
+                           const int* __restrict__ len, const int* __restrict__ bcon,
+                           const int* __restrict__ ptype, const double* __restrict__ x,
+                           const double* __restrict__ y, const double* __restrict__ z,
+                           const double* __restrict__ nsrc, int warm, double* __restrict__ pnew,
+                           int* __restrict__ mcol, double* __restrict__ mval,
+                           int* __restrict__ mlen, double* __restrict__ diag,
+                           double* __restrict__ source)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int bi = bcon[i];
+    if (bi != 0) {
+        mlen[i] = 0;
+        diag[i] = 0.0;
+        source[i] = 0.0;
+        pnew[i] = 0.0;
+        return;
+    }
+    double xi = x[i], yi = y[i], zi = DIM == 3 ? z[i] : 0.0;
+    double dg = 0.0;
+    int cnt = 0, L = len[i];
+    for (int k = 0; k < L; k++) {
+        int j = nbr[(size_t)k * pitch + i];
+        if (i == j) continue;
+        int bj = bcon[j];
+        if (bj == -1) continue;
+        double d = sqrt(dist2<DIM>(x[j] - xi, y[j] - yi, DIM == 3 ? z[j] - zi : 0.0));
+        if (fabs(d) <= 1.0e-15) continue;
+        double v;
+        if (A.matopt) {
+            v = (DIM == 2) ? 3.0 * A.re : 2.0 * A.re;
+            v = v / (d * d * d);
+            v = v / A.n0_l;
+            v = v / A.rho;
+        } else {
+            v = 2.0 * DIM / A.lambda * kernel_w(d, A.ktype, DIM, A.re) / A.n0_l / A.rho;
+        }
+        dg += v;
+        if (bj == 0 && v != 0.0) {
+            mcol[(size_t)cnt * pitch + i] = j;
+            mval[(size_t)cnt * pitch + i] = -v;
+            cnt++;
+        }
+    }
+    dg += (1.00e-7) / A.dt / A.dt;
+    diag[i] = dg;
+    mlen[i] = cnt;
+    if (!A.srcopt) source[i] = 1.0 / A.dt / A.dt * (nsrc[i] - A.n0_s) / A.n0_s;
+    if (!warm) pnew[i] = 0.0;
+}
+
+// HS + ECS source (functions.cu:924-988) is a sequential recurrence over
+// particle ids (source[i-1]); it runs as one thread walking the ids.
+template <int DIM>
+__global__ void k_source_hs(int n, int pitch, double re, double n0, double dt,
+                            const int* __restrict__ inv_id, const int* __restrict__ nbr,
+                            const int* __restrict__ len, const int* __restrict__ bcon,
+                            const int* __restrict__ ptype, const double* __restrict__ nstar,
+                            const double* __restrict__ x, const double* __restrict__ y,
+                            const double* __restrict__ z, const double* __restrict__ u,
+                            const double* __restrict__ v, const double* __restrict__ w,
+                            double* __restrict__ source)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double prev = 0.0;  // source of the previous id (0 unless written this call)
+    for (int id = 0; id < n; id++) {
+        int i = inv_id[id];
+        double out = source[i];
+        if (ptype[i] == -1) {
+            prev = 0.0;
+            continue;
+        }
+        if (bcon[i] == 0) {
+            double alpha = 0.0, beta = 0.0, ECS = 0.0;
+            if (id > 0) {
+                alpha = (nstar[i] - n0) / n0;
+                beta = (dt / n0) * (prev / (-1.0 / (n0 * dt)));
+                ECS = fabs(alpha) * (beta / dt) + fabs(beta) * (alpha / dt);
+            }
+            double sum = 0.0;
+            for (int k = 0; k < len[i]; k++) {
+                int j = nbr[(size_t)k * pitch + i];
+                if (ptype[j] <= -1 || i == j) continue;
+                double d = sqrt(dist2<DIM>(x[j] - x[i], y[j] - y[i], DIM == 3 ? z[j] - z[i] : 0.0));
+                if (fabs(d) <= 1.0e-15) continue;
+                double du = u[i] - u[j], dv = v[i] - v[j];
+                if (DIM == 3) {
+                    double dw = w[i] - w[j];
+                    sum += (re / (d * d * d)) *
+                           ((x[i] - x[j]) * du + (y[i] - y[j]) * dv + (z[i] - z[j]) * dw);
+                } else {
+                    sum += (re / (d * d * d)) * ((x[i] - x[j]) * du + (y[i] - y[j]) * dv);
+                }
+            }
+            out = (-1.25 / (n0 * dt)) * sum + ECS;
+            if (fabs(out) < 0.99) out = 0;
+        } else if (bcon[i] == 1) {
+            out = 0.0;
+        } else {
+            out = 0.0;
+        }
+        source[i] = out;
+        prev = out;
+    }
+}
+
+struct CG {
+    const int* __restrict__ mcol;
+    const double* __restrict__ mval;
+    const int* __restrict__ mlen;
+    const double* __restrict__ diag;
+    const int* __restrict__ bcon;
+    int pitch, n, precond;
+};
+
+__device__ __forceinline__ double spmv_row(const CG& A, const double* __restrict__ v, int i)
+{
+    double acc = A.diag[i] * v[i];
+    int L = A.mlen[i];
+    for (int k = 0; k < L; k++) {
+        size_t e = (size_t)k * A.pitch + i;
+        acc = acc + A.mval[e] * v[A.mcol[e]];
+    }
+    return acc;
+}
+
+// r = b - A x, z = M^-1 r, p = z; partials of b.b, r.z, r.r
+__global__ void k_cg_start(CG A, const double* __restrict__ b, const double* __restrict__ x,
+                           double* __restrict__ r, double* __restrict__ zv, double* __restrict__ p,
+                           double* __restrict__ part)
+{
+    __shared__ double sh[33];
+    double bb = 0, rz = 0, rr = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+        double ri = 0, zi = 0;
+        if (A.bcon[i] == 0) {
+            double bi = b[i];
+            ri = bi - spmv_row(A, x, i);
+            zi = A.precond ? ri / A.diag[i] : ri;
+            bb += bi * bi;
+            rz += ri * zi;
+            rr += ri * ri;
+        }
+        r[i] = ri;
+        zv[i] = zi;
+        p[i] = zi;
+    }
+    bb = block_sum(bb, sh);
+    rz = block_sum(rz, sh);
+    rr = block_sum(rr, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = bb;
+        part[gridDim.x + blockIdx.x] = rz;
+        part[2 * gridDim.x + blockIdx.x] = rr;
+    }
+}
+
+__global__ void k_cg_start_scalars(int nparts, const double* __restrict__ part, double tol2,
+                                   double* scal, int* flag)
+{
+    __shared__ double sh[33];
+    double bb = reduce_parts(part, nparts, sh);
+    double rz = reduce_parts(part + nparts, nparts, sh);
+    double rr = reduce_parts(part + 2 * nparts, nparts, sh);
+    if (threadIdx.x == 0) {
+        scal[S_BB] = bb;
+        scal[S_RZ] = rz;
+        scal[S_RR] = rr;
+        scal[S_ZERO] = (bb == 0.0) ? 1.0 : 0.0;
+        flag[0] = (bb == 0.0 || rr <= tol2 * bb) ? 1 : 0;
+        flag[1] = 0;
+    }
+}
+
+// s = A p and partial p.s
+__global__ void k_cg_spmv(CG A, const double* __restrict__ p, double* __restrict__ s,
+                          double* __restrict__ part, const int* __restrict__ flag)
+{
+    __shared__ double sh[33];
+    if (flag[0]) return;
+    double ps = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+        double si = 0;
+        if (A.bcon[i] == 0) {
+            si = spmv_row(A, p, i);
+            ps += p[i] * si;
+        }
+        s[i] = si;
+    }
+    ps = block_sum(ps, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = ps;
+}
+
+// alpha = rz / p.s; x += alpha p; r -= alpha s; z = M^-1 r; partials r.z, r.r
+__global__ void k_cg_update(CG A, double* __restrict__ x, double* __restrict__ r,
+                            double* __restrict__ zv, const double* __restrict__ p,
+                            const double* __restrict__ s, const double* __restrict__ part_ps,
+                            double* __restrict__ part, const double* __restrict__ scal,
+                            const int* __restrict__ flag)
+{
+    __shared__ double sh[33];
+    if (flag[0]) return;
+    double ps = reduce_parts(part_ps, gridDim.x, sh);
+    double alpha = scal[S_RZ] / ps;
+    double rz = 0, rr = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+        if (A.bcon[i] != 0) continue;
+        double xi = x[i] + alpha * p[i];
+        double ri = r[i] - alpha * s[i];
+        double zi = A.precond ? ri / A.diag[i] : ri;
+        x[i] = xi;
+        r[i] = ri;
+        zv[i] = zi;
+        rz += ri * zi;
+        rr += ri * ri;
+    }
+    rz = block_sum(rz, sh);
+    rr = block_sum(rr, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = rz;
+        part[gridDim.x + blockIdx.x] = rr;
+    }
+}
+
+// beta = rz'/rz; p = z + beta p.  Every block reaches the same decision from
+// the same partials; block 0 stages rz', r.r and the decision for k_cg_commit
+// (nothing read by this kernel is written by it).
+__global__ void k_cg_direction(CG A, const double* __restrict__ zv, double* __restrict__ p,
+                               const double* __restrict__ part, double* scal,
+                               const int* __restrict__ flag, double tol2, int maxit)
+{
+    __shared__ double sh[33];
+    if (flag[0]) return;
+    double rz = reduce_parts(part, gridDim.x, sh);
+    double rr = reduce_parts(part + gridDim.x, gridDim.x, sh);
+    double beta = rz / scal[S_RZ];
+    int it = flag[1] + 1;
+    bool done = (rr <= tol2 * scal[S_BB]) || it >= maxit || !(rr == rr);
+    if (!done) {
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x)
+            if (A.bcon[i] == 0) p[i] = zv[i] + beta * p[i];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        scal[S_NEWRZ] = rz;
+        scal[S_NEWRR] = rr;
+        scal[S_DONE] = done ? 1.0 : 0.0;
+    }
+}
+
+__global__ void k_invert(int n, const int* __restrict__ oid, int* __restrict__ inv_id)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) inv_id[oid[i]] = i;
+}
+
+__global__ void k_cg_commit(double* scal, int* flag)
+{
+    if (flag[0]) return;
+    scal[S_RZ] = scal[S_NEWRZ];
+    scal[S_RR] = scal[S_NEWRR];
+    flag[1] += 1;
+    if (scal[S_DONE] != 0.0) flag[0] = 1;
+}
+
+// clamp (functions.cu:2534-2547); a zero right-hand side gives p = 0
+__global__ void k_clamp(int n, double pmin, double pmax, const double* __restrict__ scal,
+                        double* __restrict__ pnew)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v = scal[S_ZERO] != 0.0 ? 0.0 : pnew[i];
+    if (v < pmin) v = pmin;
+    if (v > pmax || v * 0.0 != 0.0) v = pmax;
+    pnew[i] = v;
+}
+
+}  // namespace
+
+int vmps_ppe(mps_ctx* c)
+{
+    const mps_config& f = c->cfg;
+    cudaStream_t st = c->stream;
+    const int n = c->n;
+    const double *ax = c->x, *ay = c->y, *az = c->z, *nsrc = c->nd;
+    if (f.ppe_at_predicted) { ax = c->xs; ay = c->ys; az = c->zs; nsrc = c->nds; }
+    Asm A{f.re_l, c->lambda_l, c->n0_l, c->n0_s, f.rho1, f.dt, f.ktype, f.matopt, f.srcopt};
+    if (f.dim == 3)
+        k_assemble<3><<<grid_blocks(n), kBlock, 0, st>>>(n, c->pitch, A, c->nbr_l, c->len_l, c->bcon,
+                                                     c->ptype, ax, ay, az, nsrc, f.warm_start,
+                                                     c->pnew, c->mcol, c->mval, c->mlen, c->diag,
+                                                     c->source);
+    else
+        k_assemble<2><<<grid_blocks(n), kBlock, 0, st>>>(n, c->pitch, A, c->nbr_l, c->len_l, c->bcon,
+                                                     c->ptype, ax, ay, az, nsrc, f.warm_start,
+                                                     c->pnew, c->mcol, c->mval, c->mlen, c->diag,
+                                                     c->source);
+    vmps_count_launch(1);
+    if (f.srcopt) {
+        // slot of particle id k: inv_id[k] (the sort's inv buffer is free here)
+        k_invert<<<grid_blocks(n), kBlock, 0, st>>>(n, c->oid, c->inv);
+        vmps_count_launch(1);
+        if (f.dim == 3)
+            k_source_hs<3><<<1, 32, 0, st>>>(n, c->pitch, f.re_s, c->n0_s, f.dt, c->inv, c->nbr_s,
+                                             c->len_s, c->bcon, c->ptype, c->nds, ax, ay, az, c->us,
+                                             c->vs, c->ws, c->source);
+        else
+            k_source_hs<2><<<1, 32, 0, st>>>(n, c->pitch, f.re_s, c->n0_s, f.dt, c->inv, c->nbr_s,
+                                             c->len_s, c->bcon, c->ptype, c->nds, ax, ay, az, c->us,
+                                             c->vs, c->ws, c->source);
+        vmps_count_launch(1);
+    }
+    CG G{c->mcol, c->mval, c->mlen, c->diag, c->bcon, c->pitch, n, f.solver == 1 ? 1 : 0};
+    int nblk = 0;
+    VMPS_CUDA(c, cudaDeviceGetAttribute(&nblk, cudaDevAttrMultiProcessorCount, c->device));
+    nblk *= 4;
+    double tol2 = f.cg_tol * f.cg_tol;
+    k_cg_start<<<nblk, kRedThreads, 0, st>>>(G, c->source, c->pnew, c->cg_r, c->cg_z, c->cg_p,
+                                             c->cg_part);
+    k_cg_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal, c->cg_flag);
+    vmps_count_launch(2);
+    const int check = 4;
+    int it = 0;
+    int nspmv = 0;
+    for (; it < f.cg_max; it++) {
+        if (c->profile) {
+            while ((int)c->ev_spmv.size() < 2 * (nspmv + 1)) {
+                cudaEvent_t e;
+                VMPS_CUDA(c, cudaEventCreate(&e));
+                c->ev_spmv.push_back(e);
+            }
+            VMPS_CUDA(c, cudaEventRecord(c->ev_spmv[2 * nspmv], st));
+        }
+        k_cg_spmv<<<nblk, kRedThreads, 0, st>>>(G, c->cg_p, c->cg_s, c->cg_part + 4 * nblk,
+                                                c->cg_flag);
+        if (c->profile) VMPS_CUDA(c, cudaEventRecord(c->ev_spmv[2 * nspmv + 1], st));
+        nspmv++;
+        k_cg_update<<<nblk, kRedThreads, 0, st>>>(G, c->pnew, c->cg_r, c->cg_z, c->cg_p, c->cg_s,
+                                                  c->cg_part + 4 * nblk, c->cg_part, c->cg_scal,
+                                                  c->cg_flag);
+        k_cg_direction<<<nblk, kRedThreads, 0, st>>>(G, c->cg_z, c->cg_p, c->cg_part, c->cg_scal,
+                                                     c->cg_flag, tol2, f.cg_max);
+        k_cg_commit<<<1, 1, 0, st>>>(c->cg_scal, c->cg_flag);
+        vmps_count_launch(4);
+        if ((it + 1) % check == 0 || it + 1 == f.cg_max) {
+            VMPS_CUDA(c, cudaMemcpyAsync(c->cg_flag_host, c->cg_flag, 2 * sizeof(int),
+                                         cudaMemcpyDeviceToHost, st));
+            VMPS_CUDA(c, cudaStreamSynchronize(st));
+            if (c->cg_flag_host[0]) break;
+        }
+    }
+    VMPS_CUDA(c, cudaMemcpyAsync(c->cg_flag_host, c->cg_flag, 2 * sizeof(int),
+                                 cudaMemcpyDeviceToHost, st));
+    VMPS_CUDA(c, cudaMemcpyAsync(c->red_host, c->cg_scal, S_COUNT * sizeof(double),
+                                 cudaMemcpyDeviceToHost, st));
+    k_clamp<<<grid_blocks(n), kBlock, 0, st>>>(n, f.pmin, f.pmax, c->cg_scal, c->pnew);
+    vmps_count_launch(1);
+    VMPS_CUDA(c, cudaStreamSynchronize(st));
+    c->cg_iters = c->cg_flag_host[1];
+    if (c->profile) {
+        // spmv launches after convergence exit at once: count the working ones
+        for (int k = 0; k < nspmv && k < c->cg_iters; k++) {
+            float ms = 0;
+            VMPS_CUDA(c, cudaEventElapsedTime(&ms, c->ev_spmv[2 * k], c->ev_spmv[2 * k + 1]));
+            c->spmv_ms += ms;
+            c->spmv_launches++;
+        }
+    }
+    double bb = c->red_host[S_BB], rr = c->red_host[S_RR];
+    c->cg_relres = bb > 0 ? sqrt(rr / bb) : 0.0;
+    if (!(c->cg_relres <= f.cg_tol)) c->host_err |= MPS_ERR_NOT_CONVERGED;
+    VMPS_CUDA(c, cudaGetLastError());
+    return MPS_OK;
+}
