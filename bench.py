@@ -114,9 +114,11 @@ def spmv_algorithmic_bytes(nnz_a: float, rows: float) -> float:
     return nnz_a * 12.0 + rows * 32.0
 
 
-def build_case():
+def build_case(scale: int = 0):
+    """The benchmark scene; scale > 0 selects the smaller 3D dam used for
+    profiling captures (config.scaled_dam3d)."""
     from voxarmps_b200 import config
-    cfg, case = config.baseline(1)
+    cfg, case = config.scaled_dam3d(scale) if scale else config.baseline(1)
     cfg = config.solver_semantics(cfg)
     cfg["cg_tol"] = 1e-8
     cfg["cg_max"] = 1000
@@ -193,7 +195,7 @@ def run_ours(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    cfg, case = build_case()
+    cfg, case = build_case(args.scale)
     n = len(case["x"])
     fp = int((case["ptype"] > 0).sum())
     s = vm.Solver(cfg, case, device=dev)
@@ -218,6 +220,7 @@ def run_ours(args):
     # ---- device-resident timed region ----
     s.set_profile(True)
     iters, ppe_ms = [], []
+    stage = {k: [] for k in ("ms_neighbors", "ms_explicit", "ms_ppe", "ms_post")}
     sampler = ClockSampler(dev)
     barrier()
     sampler.start()
@@ -229,6 +232,8 @@ def run_ours(args):
         status |= s.step()
         iters.append(s.scalar("cg_iters"))
         ppe_ms.append(s.scalar("ms_ppe"))
+        for k in stage:
+            stage[k].append(s.scalar(k))
     e1.record(stream)
     barrier()
     launches = int(s.scalar("launches") - l0)
@@ -279,6 +284,7 @@ def run_ours(args):
             "fluid_particle_steps_per_s": fp * args.steps * ws / (el_ms * 1e-3),
             "ppe_ms_per_step": statistics.mean(ppe_ms), "cg_iters_mean": statistics.mean(iters),
             "cg_relres_last": relres, "status_bits": status,
+            "stage_ms": {k[3:]: statistics.mean(v) for k, v in stage.items()},
             "roofline": {"kernel": "k_cg_spmv (PPE SpMV, FP64 slot-major ELL)", "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
@@ -305,6 +311,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=int, default=0,
+                    help="profiling only: smaller 3D dam (10s x 20s x 10s fluid)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)

@@ -83,23 +83,6 @@ Grid make_grid(const mps_config& f, double re)
     return g;
 }
 
-// 2D: sqrt(d2) < re  <=>  d2 < cut  (cut = least d2 with sqrt(d2) >= re).
-// 3D: sqrt(d2) <= c  <=>  d2 <= cut (cut = greatest d2 with sqrt(d2) <= c).
-// sqrt is correctly rounded on the host and on the device, so both sides
-// take identical decisions.
-double sqrt_cut(double c, bool strict)
-{
-    double s = c * c;
-    if (strict) {
-        while (std::sqrt(s) < c) s = std::nextafter(s, INFINITY);
-        while (s > 0 && std::sqrt(std::nextafter(s, 0.0)) >= c) s = std::nextafter(s, 0.0);
-    } else {
-        while (std::sqrt(s) > c) s = std::nextafter(s, 0.0);
-        while (std::sqrt(std::nextafter(s, INFINITY)) <= c) s = std::nextafter(s, INFINITY);
-    }
-    return s;
-}
-
 int lattice_count(int dim, double ratio, bool inclusive)
 {
     int r = (int)std::ceil(ratio) + 1, cnt = 0;
@@ -113,6 +96,7 @@ int lattice_count(int dim, double ratio, bool inclusive)
     return cnt;
 }
 
+// row capacity: 1.5x the lattice count plus slack, rows 32-byte aligned
 int auto_cap(const mps_config& f, double re)
 {
     bool three = f.dim == 3;
@@ -217,27 +201,37 @@ int allocate(mps_ctx* c)
                           &c->phat, &c->un, &c->vn, &c->wn, &c->rho, &c->nd, &c->xs, &c->ys,
                           &c->zs, &c->us, &c->vs, &c->ws, &c->nds, &c->C, &c->meu, &c->neut,
                           &c->t1, &c->t2, &c->t3, &c->source, &c->diag, &c->cg_r, &c->cg_z,
-                          &c->cg_p, &c->cg_s, &c->xc, &c->yc, &c->zc, &c->uc, &c->vc, &c->wc};
+                          &c->cg_p, &c->cg_s, &c->xc, &c->yc, &c->zc, &c->uc, &c->vc, &c->wc,
+                          &c->pres_x, &c->pres_y, &c->pres_z};
     for (auto f : dfields) TRY(dalloc(c, f, P));
     int** ifields[] = {&c->ptype, &c->oid, &c->bcon, &c->cell_l, &c->cell_s, &c->bpos_l,
                        &c->bpos_s, &c->bslot_l, &c->boid_l, &c->bslot_s, &c->boid_s, &c->src,
-                       &c->inv, &c->perm_s, &c->perm_s_tmp, &c->len_l, &c->len_s, &c->mlen};
+                       &c->inv, &c->perm_s, &c->perm_s_tmp, &c->len_l, &c->len_s, &c->mlen,
+                       &c->moff};
     for (auto f : ifields) TRY(dalloc(c, f, P));
     TRY(dalloc(c, &c->S6, 6 * P));
     TRY(dalloc(c, &c->stage_in, P));
+    TRY(dalloc(c, &c->P4, P));
+    TRY(dalloc(c, &c->P4s, P));
+    TRY(dalloc(c, &c->P4c, P));
+    TRY(dalloc(c, &c->U4, P));
+    TRY(dalloc(c, &c->PH, P));
     TRY(dalloc(c, &c->cnt_l, (size_t)c->gl.tnc + 2));
     TRY(dalloc(c, &c->cst_l, (size_t)c->gl.tnc + 2));
     TRY(dalloc(c, &c->cnt_s, (size_t)c->gs.tnc + 2));
     TRY(dalloc(c, &c->cst_s, (size_t)c->gs.tnc + 2));
-    size_t tiles = (size_t)std::max(c->gl.tnc, c->gs.tnc) / 8192 + 4;
+    size_t tiles = (size_t)std::max(std::max(c->gl.tnc, c->gs.tnc), c->n) / 8192 + 4;
     TRY(dalloc(c, &c->scan_tmp, tiles));
+    // row-major lists and matrix: row i at i * cap
     TRY(dalloc(c, &c->nbr_l, (size_t)c->cap_l * P));
     TRY(dalloc(c, &c->nbr_s, (size_t)c->cap_s * P));
     TRY(dalloc(c, &c->mcol, (size_t)c->cap_l * P));
     TRY(dalloc(c, &c->mval, (size_t)c->cap_l * P));
     int sms = 0;
     VMPS_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-    TRY(dalloc(c, &c->cg_part, (size_t)8 * 4 * sms + 64));
+    // CG partials: 5 arrays of one value per block, at most 8 blocks per SM
+    c->cg_part_cap = (size_t)5 * 8 * sms;
+    TRY(dalloc(c, &c->cg_part, c->cg_part_cap));
     TRY(dalloc(c, &c->cg_scal, 16));
     TRY(dalloc(c, &c->cg_flag, 4));
     TRY(dalloc(c, &c->d_err, 1));
@@ -361,8 +355,8 @@ int mps_upload(mps_ctx* c, int n, const double* x, const double* y, const double
     bool strict = f.dim == 2;
     c->cut_l = sqrt_cut(strict ? f.re_l : f.re_l + f.delta, strict);
     c->cut_s = sqrt_cut(strict ? f.re_s : f.re_s + f.delta, strict);
-    c->cap_l = f.list_cap_l > 0 ? f.list_cap_l : auto_cap(f, f.re_l);
-    c->cap_s = f.list_cap_s > 0 ? f.list_cap_s : auto_cap(f, f.re_s);
+    c->cap_l = f.list_cap_l > 0 ? (f.list_cap_l + 7) / 8 * 8 : auto_cap(f, f.re_l);
+    c->cap_s = f.list_cap_s > 0 ? (f.list_cap_s + 7) / 8 * 8 : auto_cap(f, f.re_s);
     c->lambda_l = 0.0;  // main.cu:491-494 at the Laplacian radius
     double re = f.re_l;
     if (f.ktype == 1) c->lambda_l = 0.22143 * (re * re);
@@ -560,6 +554,7 @@ int mps_set_state(mps_ctx* c, const double* x, const double* y, const double* z,
                                                                k == 6 ? c->pnew : nullptr);
         vmps_count_launch(1);
     }
+    TRY(vmps_pack(c));
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
 }
@@ -627,25 +622,49 @@ int mps_download_lists(mps_ctx* c, int which, int* off, int* nbr, long* total)
     if (!c || c->n == 0 || (which != 0 && which != 1)) return MPS_ERR_ARG;
     VMPS_CUDA(c, cudaSetDevice(c->device));
     const int n = c->n, P = c->pitch;
-    int cap = which == 0 ? c->cap_s : c->cap_l;
+    int cap = which == 0 ? c->cap_s : c->cap_l;  // rows i*cap .. i*cap+len-1
     const int* dl = which == 0 ? c->len_s : c->len_l;
     const int* dn = which == 0 ? c->nbr_s : c->nbr_l;
-    std::vector<int> len(n), oid(n), ent((size_t)cap * P);
+    std::vector<int> len(n), oid(n), cell(n), ent((size_t)cap * P);
     VMPS_CUDA(c, cudaMemcpy(len.data(), dl, sizeof(int) * n, cudaMemcpyDeviceToHost));
     VMPS_CUDA(c, cudaMemcpy(oid.data(), c->oid, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    VMPS_CUDA(c, cudaMemcpy(cell.data(), which == 0 ? c->cell_s : c->cell_l, sizeof(int) * n,
+                            cudaMemcpyDeviceToHost));
     VMPS_CUDA(c, cudaMemcpy(ent.data(), dn, sizeof(int) * ent.size(), cudaMemcpyDeviceToHost));
+    const Grid& g = which == 0 ? c->gs : c->gl;
     std::vector<int> slot_of(n);
     for (int i = 0; i < n; i++) slot_of[oid[i]] = i;
     long tot = 0;
     for (int q = 0; q < n; q++) tot += len[slot_of[q]];
     if (total) *total = tot;
     if (!off) return MPS_OK;
+    // rows are stored in scan order; the reference's order is x offset
+    // outermost, then y, then z, ascending id inside a cell (functions.cu:2858)
+    auto coords = [&](int C, int& a, int& b, int& k) {
+        C -= 1;
+        a = C % g.ncx;
+        b = (C / g.ncx) % g.ncy;
+        k = C / (g.ncx * g.ncy);
+    };
+    std::vector<std::pair<long, int>> keyed;
     long acc = 0;
     for (int q = 0; q < n; q++) {
         int i = slot_of[q];
         off[q] = (int)acc;
-        if (nbr)
-            for (int k = 0; k < len[i]; k++) nbr[acc + k] = oid[ent[(size_t)k * P + i]];
+        if (nbr) {
+            int ai, bi, ki;
+            coords(cell[i], ai, bi, ki);
+            keyed.clear();
+            for (int k = 0; k < len[i]; k++) {
+                int j = ent[(size_t)i * cap + k];
+                int aj, bj, kj;
+                coords(cell[j], aj, bj, kj);
+                long rank = (long)(aj - ai + 1) * 9 + (bj - bi + 1) * 3 + (kj - ki + 1);
+                keyed.emplace_back(rank * (long)n + oid[j], oid[j]);
+            }
+            std::sort(keyed.begin(), keyed.end());
+            for (int k = 0; k < len[i]; k++) nbr[acc + k] = keyed[k].second;
+        }
         acc += len[i];
     }
     off[n] = (int)acc;

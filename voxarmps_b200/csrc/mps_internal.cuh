@@ -4,13 +4,16 @@
 // Layout in HBM: structure-of-arrays, particles in cell order (re-sorted
 // every step by (cell, original id), the order NEIGHBOR's counting sort
 // produces, functions.cu:2820-2852).  Neighbour lists and the PPE matrix are
-// slot-major ELL: entry k of row i lives at k * pitch + i, so a warp of 32
-// consecutive rows reads 128 contiguous bytes per slot.
+// row-major with a fixed row capacity: entry k of row i lives at i*cap + k.
+// Kernels over the Laplacian-radius list (about 300 entries per row in 3D)
+// give each row a whole warp; kernels over the PND-radius list (about 50)
+// give each row a group of GS lanes; either way a row streams contiguously.
 #pragma once
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -39,6 +42,42 @@ struct Cutoff {
 struct DeviceError {
     unsigned int bits;
 };
+
+// 2D cutoffs:  sqrt(d2) <  c  <=>  d2 <  sqrt_cut(c, true)
+// 3D cutoffs:  sqrt(d2) <= c  <=>  d2 <= sqrt_cut(c, false)
+// sqrt is correctly rounded on the host and on the device, so comparing the
+// squared distance with these thresholds takes the reference's decisions.
+inline double sqrt_cut(double c, bool strict)
+{
+    double s = c * c;
+    if (strict) {
+        while (std::sqrt(s) < c) s = std::nextafter(s, INFINITY);
+        while (s > 0 && std::sqrt(std::nextafter(s, 0.0)) >= c) s = std::nextafter(s, 0.0);
+    } else {
+        while (std::sqrt(s) > c) s = std::nextafter(s, 0.0);
+        while (std::sqrt(std::nextafter(s, INFINITY)) <= c) s = std::nextafter(s, INFINITY);
+    }
+    return s;
+}
+
+// Kernel function W() of one radius in the form the stage kernels evaluate:
+// support tests on d2 against exact thresholds (q < 1 <=> d2 < lt, q <= 1
+// <=> d2 <= le), magnitudes from rD = rsqrt(d2).
+struct WK {
+    double re, inv_re, lt, le;
+    int ktype;
+};
+
+inline WK make_wk(int ktype, double re)
+{
+    WK k;
+    k.re = re;
+    k.inv_re = 1.0 / re;
+    k.lt = sqrt_cut(re, true);
+    k.le = sqrt_cut(re, false);
+    k.ktype = ktype;
+    return k;
+}
 
 }  // namespace vmps
 
@@ -73,6 +112,10 @@ struct mps_ctx {
     double* S6 = nullptr;
     double *xc = nullptr, *yc = nullptr, *zc = nullptr, *uc = nullptr, *vc = nullptr,
            *wc = nullptr;
+    // packed gathers: positions (x, y, z, ptype), predicted positions,
+    // collision output, velocities (u, v, w, -) and (pnew, phat) pairs
+    double4 *P4 = nullptr, *P4s = nullptr, *P4c = nullptr, *U4 = nullptr;
+    double2* PH = nullptr;
     // sort / cells
     int *cell_l = nullptr, *cell_s = nullptr;      // per slot, 1-based Cnum
     int *bpos_l = nullptr, *bpos_s = nullptr;      // position inside the bucket
@@ -85,10 +128,12 @@ struct mps_ctx {
     // lists (slot-major)
     int *nbr_l = nullptr, *len_l = nullptr, *nbr_s = nullptr, *len_s = nullptr;
     // PPE matrix (compact slot-major ELL) and CG vectors
-    int *mcol = nullptr, *mlen = nullptr;
+    int *mcol = nullptr, *mlen = nullptr, *moff = nullptr;  // CSR: row i at moff[i]
     double* mval = nullptr;
+    double *pres_x = nullptr, *pres_y = nullptr, *pres_z = nullptr;  // prediction pressure sums
     double *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_s = nullptr;
     double* cg_part = nullptr;   // block partial sums
+    size_t cg_part_cap = 0;      // doubles in cg_part
     double* cg_scal = nullptr;   // device scalars (rz, bb, rr, ...)
     int* cg_flag = nullptr;      // [0] done, [1] iterations
     int* cg_flag_host = nullptr; // pinned
@@ -191,6 +236,75 @@ __device__ __forceinline__ bool cell_coords(const Grid& g, double x, double y, d
 
 inline int grid_blocks(long n) { return (int)((n + kBlock - 1) / kBlock); }
 
+// W() of functions.cu:32-74 from d2 and rD = rsqrt(d2)
+template <int DIM>
+__device__ __forceinline__ double w_fast(const WK& k, double d2, double rD)
+{
+    if (k.ktype == 2) return d2 < k.lt ? k.re * rD - 1.0 : 0.0;
+    double R = d2 * rD, q = R * k.inv_re;
+    switch (k.ktype) {
+    case 6:
+        if (d2 <= k.le) {
+            double t = 1.0 - q;
+            return t * t * t;
+        }
+        return 0.0;
+    case 1:
+        if (q < 0.5) return 2.0 - 4.0 * (q * q);
+        if (d2 <= k.le) {
+            double t = 2 * q - 2;
+            return t * t;
+        }
+        return 0.0;
+    case 5:
+        return d2 <= k.le ? 1.5 * log(1 / (q + 0.000001)) : 0.0;
+    default:
+        return kernel_w(R, k.ktype, DIM, k.re);
+    }
+}
+
+__device__ __forceinline__ double rsq(double d2) { return rsqrt(d2); }
+
+// A group of G consecutive lanes (G divides 32) that cooperates on one row.
+template <int G>
+struct Grp {
+    int lane;       // 0..G-1
+    long gid;       // global group index
+    unsigned mask;  // this group's lanes inside the warp
+    unsigned base;  // first warp lane of the group
+    __device__ __forceinline__ Grp()
+    {
+        long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+        lane = (int)(t % G);
+        gid = t / G;
+        base = (threadIdx.x & 31u) - (unsigned)lane;
+        mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << base);
+    }
+    // sum over the group, result in every lane (fixed butterfly order)
+    __device__ __forceinline__ double sum(double v) const
+    {
+        for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+        return v;
+    }
+    __device__ __forceinline__ double min(double v) const
+    {
+        for (int o = G / 2; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(mask, v, o));
+        return v;
+    }
+    // ballot restricted to the group, bit k = group lane k
+    __device__ __forceinline__ unsigned ballot(bool p) const
+    {
+        unsigned m = __ballot_sync(mask, p);
+        return (G == 32) ? m : (m >> base) & ((1u << G) - 1u);
+    }
+};
+
+// lanes per PND-radius row
+template <int DIM>
+struct SmallG {
+    static constexpr int G = DIM == 3 ? 8 : 4;
+};
+
 }  // namespace vmps
 
 // host-side helpers implemented in mps_context.cu
@@ -218,3 +332,5 @@ int vmps_integrate(mps_ctx* ctx);
 int vmps_collision(mps_ctx* ctx);
 int vmps_commit(mps_ctx* ctx);
 int vmps_count_launch(int k);
+int vmps_pack(mps_ctx* ctx);
+int vmps_scan(mps_ctx* ctx, int m, const int* in, int* out);

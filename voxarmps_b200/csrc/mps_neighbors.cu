@@ -13,7 +13,8 @@
 //   5. k_gather    reorder the persistent particle state into cell order;
 //   6. k_lists     both lists in the reference's scan order (row, colu, dep;
 //                  ascending id inside a cell), membership decided with the
-//                  reference's exact FP64 arithmetic.
+//                  reference's exact FP64 arithmetic; a warp per particle for
+//                  the Laplacian radius, GS lanes for the PND radius.
 #include <cstdio>
 
 #include "mps_internal.cuh"
@@ -194,56 +195,86 @@ __global__ void k_translate(int n, const int* __restrict__ inv, const int* __res
     if (k < n) out[k] = inv[in[k]];
 }
 
-// Both lists, one thread per particle (reference scan order; see file head).
-template <int DIM>
-__global__ void k_lists(int n, int pitch, Grid gl, Grid gs, double cut_l, double cut_s,
-                        int cap_l, int cap_s, const double* __restrict__ x,
-                        const double* __restrict__ y, const double* __restrict__ z,
-                        const int* __restrict__ cell_l, const int* __restrict__ cell_s,
-                        const int* __restrict__ cst_l, const int* __restrict__ cnt_l,
-                        const int* __restrict__ cst_s, const int* __restrict__ cnt_s,
-                        const int* __restrict__ perm_s, int* __restrict__ nbr_l,
-                        int* __restrict__ len_l, int* __restrict__ nbr_s, int* __restrict__ len_s,
-                        int* len_max, unsigned int* err)
+// One list, G lanes per particle, row-major.  Membership is the reference's
+// exact FP64 rule (3D: d <= cut, self included; 2D: d < cut, self excluded)
+// over the 3x3(x3) cells around the particle's cell (functions.cu:2854-2918).
+// The three cells of one (y, z) offset are consecutive in memory (cells are
+// numbered x fastest and particles are stored in cell order), so they are
+// scanned as one range; cells whose box lies farther than the cutoff from
+// the particle are left out of the range (conservative margin).  Rows are
+// stored in scan order (y, z outer, memory order inside); the reference's
+// own order (x offset outermost, ascending id per cell) is restored when
+// lists are exported (mps_download_lists).
+template <int DIM, int G>
+__global__ void k_lists(int n, Grid g, double cut, int cap, const double4* __restrict__ P4,
+                        const int* __restrict__ cell, const int* __restrict__ cst,
+                        const int* __restrict__ cnt, const int* __restrict__ perm,
+                        int* __restrict__ out, int* __restrict__ len, int* len_max, int which,
+                        unsigned int* err)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double xi = x[i], yi = y[i], zi = DIM == 3 ? z[i] : 0.0;
-    for (int pass = 0; pass < 2; pass++) {
-        const Grid& g = pass == 0 ? gl : gs;
-        int C = (pass == 0 ? cell_l[i] : cell_s[i]) - 1;
-        int ic = C % g.ncx + 1, jc = (C / g.ncx) % g.ncy + 1, kc = C / (g.ncx * g.ncy) + 1;
-        int m1 = (ic == 1) ? 0 : -1, m2 = (ic == g.ncx) ? 0 : 1;
-        int m3 = (jc == 1) ? 0 : -1, m4 = (jc == g.ncy) ? 0 : 1;
-        int m5 = 0, m6 = 0;
-        if (DIM == 3) { m5 = (kc == 1) ? 0 : -1; m6 = (kc == g.ncz) ? 0 : 1; }
-        const int* cst = pass == 0 ? cst_l : cst_s;
-        const int* cnt = pass == 0 ? cnt_l : cnt_s;
-        int* out = pass == 0 ? nbr_l : nbr_s;
-        int cap = pass == 0 ? cap_l : cap_s;
-        double cut = pass == 0 ? cut_l : cut_s;
-        int k = 0;
-        for (int row = m1; row <= m2; row++)
-            for (int colu = m3; colu <= m4; colu++)
-                for (int dep = m5; dep <= m6; dep++) {
-                    int Cn = ic + row + (jc - 1 + colu) * g.ncx + (kc - 1 + dep) * g.ncx * g.ncy;
-                    int b = cst[Cn], e = b + cnt[Cn];
-                    for (int jj = b; jj < e; jj++) {
-                        int j = pass == 0 ? jj : perm_s[jj];
-                        double d2 = dist2<DIM>(x[j] - xi, y[j] - yi, DIM == 3 ? z[j] - zi : 0.0);
-                        bool in = (DIM == 3) ? (d2 <= cut) : (j != i && d2 < cut);
-                        if (in) {
-                            if (k < cap) out[(size_t)k * pitch + i] = j;
-                            k++;
-                        }
-                    }
+    Grp<G> q;
+    int i = (int)q.gid;
+    if (i >= n) return;  // whole groups leave together (n rows, G lanes each)
+    double4 pi = P4[i];
+    int C = cell[i] - 1;
+    int ic = C % g.ncx + 1, jc = (C / g.ncx) % g.ncy + 1, kc = C / (g.ncx * g.ncy) + 1;
+    int m1 = (ic == 1) ? 0 : -1, m2 = (ic == g.ncx) ? 0 : 1;
+    int m3 = (jc == 1) ? 0 : -1, m4 = (jc == g.ncy) ? 0 : 1;
+    int m5 = 0, m6 = 0;
+    if (DIM == 3) { m5 = (kc == 1) ? 0 : -1; m6 = (kc == g.ncz) ? 0 : 1; }
+    // distances from the particle to the faces of its own cell; a margin of
+    // 1e-9 cell sizes keeps the culling conservative under rounding
+    const double mx = 1e-9 * g.re, mz = 1e-9 * g.rez;
+    double lox = pi.x - (g.xmin + (ic - 1) * g.re) - mx, hix = (g.xmin + ic * g.re) - pi.x - mx;
+    double loy = pi.y - (g.ymin + (jc - 1) * g.re) - mx, hiy = (g.ymin + jc * g.re) - pi.y - mx;
+    double loz = 0, hiz = 0;
+    if (DIM == 3) {
+        loz = pi.z - (g.zmin + (kc - 1) * g.rez) - mz;
+        hiz = (g.zmin + kc * g.rez) - pi.z - mz;
+    }
+    auto gap2 = [](int off, double lo, double hi) {
+        double d = off < 0 ? lo : (off > 0 ? hi : 0.0);
+        return d > 0 ? d * d : 0.0;
+    };
+    const double gxl = gap2(-1, lox, hix), gxh = gap2(1, lox, hix);
+    int* row = out + (size_t)i * cap;
+    int k = 0;
+    for (int cu = m3; cu <= m4; cu++) {
+        double gy = gap2(cu, loy, hiy);
+        for (int dp = m5; dp <= m6; dp++) {
+            double gyz = gy + (DIM == 3 ? gap2(dp, loz, hiz) : 0.0);
+            if (gyz > cut) continue;
+            int rlo = (m1 < 0 && gyz + gxl <= cut) ? -1 : 0;
+            int rhi = (m2 > 0 && gyz + gxh <= cut) ? 1 : 0;
+            int Cr = ic + (jc - 1 + cu) * g.ncx + (kc - 1 + dp) * g.ncx * g.ncy;
+            int b = cst[Cr + rlo], e = cst[Cr + rhi] + cnt[Cr + rhi];
+            for (int base = b; base < e; base += G) {
+                int jj = base + q.lane;
+                bool in = false;
+                int j = 0;
+                if (jj < e) {
+                    j = perm ? perm[jj] : jj;
+                    double4 pj = P4[j];
+                    double d2 = dist2<DIM>(pj.x - pi.x, pj.y - pi.y,
+                                           DIM == 3 ? pj.z - pi.z : 0.0);
+                    in = (DIM == 3) ? (d2 <= cut) : (j != i && d2 < cut);
                 }
+                unsigned m = q.ballot(in);
+                if (in) {
+                    int pos = k + __popc(m & ((1u << q.lane) - 1u));
+                    if (pos < cap) row[pos] = j;
+                }
+                k += __popc(m);
+            }
+        }
+    }
+    if (q.lane == 0) {
+        atomicMax(&len_max[which], k);
         if (k > cap) {
             set_error(err, MPS_ERR_LIST_OVERFLOW);
             k = cap;
         }
-        (pass == 0 ? len_l : len_s)[i] = k;
-        atomicMax(&len_max[pass], k);
+        len[i] = k;
     }
 }
 
@@ -258,6 +289,11 @@ int scan(mps_ctx* ctx, int m, const int* in, int* out, int* tile_sum)
 }
 
 }  // namespace
+
+int vmps_scan(mps_ctx* ctx, int m, const int* in, int* out)
+{
+    return scan(ctx, m, in, out, ctx->scan_tmp);
+}
 
 // Persistent fields carried through the reorder (all other fields are
 // recomputed each step before use).
@@ -328,22 +364,34 @@ int vmps_neighbors(mps_ctx* ctx)
     }
     k_translate<<<nb, kBlock, 0, st>>>(n, ctx->inv, ctx->perm_s_tmp, ctx->perm_s);
     vmps_count_launch(1);
+    {
+        int r = vmps_pack(ctx);
+        if (r != MPS_OK) return r;
+    }
     if (ctx->profile) VMPS_CUDA(ctx, cudaEventRecord(ctx->ev[6], st));
-    if (ctx->cfg.dim == 3)
-        k_lists<3><<<nb, kBlock, 0, st>>>(n, ctx->pitch, ctx->gl, ctx->gs, ctx->cut_l, ctx->cut_s,
-                                          ctx->cap_l, ctx->cap_s, ctx->x, ctx->y, ctx->z,
-                                          ctx->cell_l, ctx->cell_s, ctx->cst_l, ctx->cnt_l,
-                                          ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_l,
-                                          ctx->len_l, ctx->nbr_s, ctx->len_s, ctx->len_max,
-                                          ctx->d_err);
-    else
-        k_lists<2><<<nb, kBlock, 0, st>>>(n, ctx->pitch, ctx->gl, ctx->gs, ctx->cut_l, ctx->cut_s,
-                                          ctx->cap_l, ctx->cap_s, ctx->x, ctx->y, ctx->z,
-                                          ctx->cell_l, ctx->cell_s, ctx->cst_l, ctx->cnt_l,
-                                          ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_l,
-                                          ctx->len_l, ctx->nbr_s, ctx->len_s, ctx->len_max,
-                                          ctx->d_err);
-    vmps_count_launch(1);
+    {
+        const int n32 = (int)(((long)n * 32 + kBlock - 1) / kBlock);
+        if (ctx->cfg.dim == 3) {
+            constexpr int GS = SmallG<3>::G;
+            k_lists<3, 32><<<n32, kBlock, 0, st>>>(n, ctx->gl, ctx->cut_l, ctx->cap_l, ctx->P4,
+                                                   ctx->cell_l, ctx->cst_l, ctx->cnt_l, nullptr,
+                                                   ctx->nbr_l, ctx->len_l, ctx->len_max, 0,
+                                                   ctx->d_err);
+            k_lists<3, GS><<<(int)(((long)n * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+                n, ctx->gs, ctx->cut_s, ctx->cap_s, ctx->P4, ctx->cell_s, ctx->cst_s, ctx->cnt_s,
+                ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1, ctx->d_err);
+        } else {
+            constexpr int GS = SmallG<2>::G;
+            k_lists<2, 32><<<n32, kBlock, 0, st>>>(n, ctx->gl, ctx->cut_l, ctx->cap_l, ctx->P4,
+                                                   ctx->cell_l, ctx->cst_l, ctx->cnt_l, nullptr,
+                                                   ctx->nbr_l, ctx->len_l, ctx->len_max, 0,
+                                                   ctx->d_err);
+            k_lists<2, GS><<<(int)(((long)n * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+                n, ctx->gs, ctx->cut_s, ctx->cap_s, ctx->P4, ctx->cell_s, ctx->cst_s, ctx->cnt_s,
+                ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1, ctx->d_err);
+        }
+    }
+    vmps_count_launch(2);
     if (ctx->profile) {
         VMPS_CUDA(ctx, cudaEventRecord(ctx->ev[7], st));
         VMPS_CUDA(ctx, cudaEventSynchronize(ctx->ev[7]));

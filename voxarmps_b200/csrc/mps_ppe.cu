@@ -48,67 +48,85 @@ __device__ __forceinline__ double reduce_parts(const double* part, int nparts, d
 }
 
 struct Asm {
-    double re, lambda, n0_l, n0_s, rho, dt;
-    int ktype, matopt, srcopt;
+    WK wk;
+    double cw;    // 2*DIM/lambda/n0_l/rho: coefficient of W (functions.cu:915)
+    double cm;    // (3 or 2)*re/n0_l/rho: HL coefficient of 1/d^3 (functions.cu:901-910)
+    double reg;   // 1e-7/dt/dt (functions.cu:921)
+    double tiny2; // fabs(d) <= 1e-15  <=>  d2 <= tiny2
+    double n0_s, dt;
+    int matopt, srcopt;
 };
 
+// one warp per row; the non-zero columns are compacted in list order into
+// the row's CSR segment (capacity = the row's list length)
 template <int DIM>
-__global__ void k_assemble(int n, int pitch, Asm A, const int* __restrict__ nbr,
+__global__ void k_assemble(int n, int cap, Asm A, const int* __restrict__ nbr,
                            const int* __restrict__ len, const int* __restrict__ bcon,
-                           const int* __restrict__ ptype, const double* __restrict__ x,
-                           const double* __restrict__ y, const double* __restrict__ z,
-                           const double* __restrict__ nsrc, int warm, double* __restrict__ pnew,
+                           const double4* __restrict__ P4, const double* __restrict__ nsrc,
+                           int warm, double* __restrict__ pnew, const int* __restrict__ moff,
                            int* __restrict__ mcol, double* __restrict__ mval,
                            int* __restrict__ mlen, double* __restrict__ diag,
                            double* __restrict__ source)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    Grp<32> q;
+    int i = (int)q.gid;
     if (i >= n) return;
     int bi = bcon[i];
     if (bi != 0) {
-        mlen[i] = 0;
-        diag[i] = 0.0;
-        source[i] = 0.0;
-        pnew[i] = 0.0;
+        if (q.lane == 0) {
+            mlen[i] = 0;
+            diag[i] = 0.0;
+            source[i] = 0.0;
+            pnew[i] = 0.0;
+        }
         return;
     }
-    double xi = x[i], yi = y[i], zi = DIM == 3 ? z[i] : 0.0;
+    double4 pi = P4[i];
+    const int* row = nbr + (size_t)i * cap;
+    int* crow = mcol + moff[i];
+    double* vrow = mval + moff[i];
     double dg = 0.0;
     int cnt = 0, L = len[i];
-    for (int k = 0; k < L; k++) {
-        int j = nbr[(size_t)k * pitch + i];
-        if (i == j) continue;
-        int bj = bcon[j];
-        if (bj == -1) continue;
-        double d = sqrt(dist2<DIM>(x[j] - xi, y[j] - yi, DIM == 3 ? z[j] - zi : 0.0));
-        if (fabs(d) <= 1.0e-15) continue;
-        double v;
-        if (A.matopt) {
-            v = (DIM == 2) ? 3.0 * A.re : 2.0 * A.re;
-            v = v / (d * d * d);
-            v = v / A.n0_l;
-            v = v / A.rho;
-        } else {
-            v = 2.0 * DIM / A.lambda * kernel_w(d, A.ktype, DIM, A.re) / A.n0_l / A.rho;
+    for (int base = 0; base < L; base += 32) {
+        int k = base + q.lane;
+        double v = 0.0;
+        int j = -1;
+        bool keep = false;
+        if (k < L) {
+            j = row[k];
+            int bj = j == i ? -1 : bcon[j];
+            if (bj != -1) {
+                double4 pj = P4[j];
+                double d2 = dist2<DIM>(pj.x - pi.x, pj.y - pi.y, DIM == 3 ? pj.z - pi.z : 0.0);
+                if (d2 > A.tiny2) {
+                    double rD = rsq(d2);
+                    v = A.matopt ? A.cm * (rD * rD * rD) : A.cw * w_fast<DIM>(A.wk, d2, rD);
+                    keep = (bj == 0 && v != 0.0);
+                }
+            }
         }
         dg += v;
-        if (bj == 0 && v != 0.0) {
-            mcol[(size_t)cnt * pitch + i] = j;
-            mval[(size_t)cnt * pitch + i] = -v;
-            cnt++;
+        unsigned m = q.ballot(keep);
+        if (keep) {
+            int pos = cnt + __popc(m & ((1u << q.lane) - 1u));
+            crow[pos] = j;
+            vrow[pos] = -v;
         }
+        cnt += __popc(m);
     }
-    dg += (1.00e-7) / A.dt / A.dt;
-    diag[i] = dg;
-    mlen[i] = cnt;
-    if (!A.srcopt) source[i] = 1.0 / A.dt / A.dt * (nsrc[i] - A.n0_s) / A.n0_s;
-    if (!warm) pnew[i] = 0.0;
+    dg = q.sum(dg);
+    if (q.lane == 0) {
+        diag[i] = dg + A.reg;
+        mlen[i] = cnt;
+        if (!A.srcopt) source[i] = 1.0 / A.dt / A.dt * (nsrc[i] - A.n0_s) / A.n0_s;
+        if (!warm) pnew[i] = 0.0;
+    }
 }
 
 // HS + ECS source (functions.cu:924-988) is a sequential recurrence over
 // particle ids (source[i-1]); it runs as one thread walking the ids.
 template <int DIM>
-__global__ void k_source_hs(int n, int pitch, double re, double n0, double dt,
+__global__ void k_source_hs(int n, int cap, double re, double n0, double dt,
                             const int* __restrict__ inv_id, const int* __restrict__ nbr,
                             const int* __restrict__ len, const int* __restrict__ bcon,
                             const int* __restrict__ ptype, const double* __restrict__ nstar,
@@ -135,7 +153,7 @@ __global__ void k_source_hs(int n, int pitch, double re, double n0, double dt,
             }
             double sum = 0.0;
             for (int k = 0; k < len[i]; k++) {
-                int j = nbr[(size_t)k * pitch + i];
+                int j = nbr[(size_t)i * cap + k];
                 if (ptype[j] <= -1 || i == j) continue;
                 double d = sqrt(dist2<DIM>(x[j] - x[i], y[j] - y[i], DIM == 3 ? z[j] - z[i] : 0.0));
                 if (fabs(d) <= 1.0e-15) continue;
@@ -164,20 +182,32 @@ struct CG {
     const int* __restrict__ mcol;
     const double* __restrict__ mval;
     const int* __restrict__ mlen;
+    const int* __restrict__ moff;
     const double* __restrict__ diag;
     const int* __restrict__ bcon;
-    int pitch, n, precond;
+    int cap, n, precond, nparts;
 };
 
-__device__ __forceinline__ double spmv_row(const CG& A, const double* __restrict__ v, int i)
+// (A v)_i with one warp on row i of the CSR matrix: two column/value loads
+// per lane in flight, gathers of v from L2, butterfly sum in a fixed order;
+// every lane returns the row's value.
+__device__ __forceinline__ double spmv_row_warp(const CG& A, const Grp<32>& q,
+                                                const double* __restrict__ v, int i)
 {
-    double acc = A.diag[i] * v[i];
-    int L = A.mlen[i];
-    for (int k = 0; k < L; k++) {
-        size_t e = (size_t)k * A.pitch + i;
-        acc = acc + A.mval[e] * v[A.mcol[e]];
+    const int L = A.mlen[i];
+    const int* __restrict__ c = A.mcol + A.moff[i];
+    const double* __restrict__ a = A.mval + A.moff[i];
+    double acc0 = 0.0, acc1 = 0.0;
+    int k = q.lane;
+    for (; k + 32 < L; k += 64) {
+        int c0 = __ldg(c + k), c1 = __ldg(c + k + 32);
+        double a0 = __ldg(a + k), a1 = __ldg(a + k + 32);
+        acc0 += a0 * v[c0];
+        acc1 += a1 * v[c1];
     }
-    return acc;
+    if (k < L) acc0 += __ldg(a + k) * v[__ldg(c + k)];
+    double acc = q.sum(acc0 + acc1);
+    return A.diag[i] * v[i] + acc;
 }
 
 // r = b - A x, z = M^-1 r, p = z; partials of b.b, r.z, r.r
@@ -186,28 +216,35 @@ __global__ void k_cg_start(CG A, const double* __restrict__ b, const double* __r
                            double* __restrict__ part)
 {
     __shared__ double sh[33];
+    Grp<32> q;
+    const long nwarps = (long)gridDim.x * blockDim.x / 32;
     double bb = 0, rz = 0, rr = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+    for (long w = q.gid; w < A.n; w += nwarps) {
+        int i = (int)w;
         double ri = 0, zi = 0;
         if (A.bcon[i] == 0) {
             double bi = b[i];
-            ri = bi - spmv_row(A, x, i);
+            ri = bi - spmv_row_warp(A, q, x, i);
             zi = A.precond ? ri / A.diag[i] : ri;
-            bb += bi * bi;
-            rz += ri * zi;
-            rr += ri * ri;
+            if (q.lane == 0) {
+                bb += bi * bi;
+                rz += ri * zi;
+                rr += ri * ri;
+            }
         }
-        r[i] = ri;
-        zv[i] = zi;
-        p[i] = zi;
+        if (q.lane == 0) {
+            r[i] = ri;
+            zv[i] = zi;
+            p[i] = zi;
+        }
     }
     bb = block_sum(bb, sh);
     rz = block_sum(rz, sh);
     rr = block_sum(rr, sh);
     if (threadIdx.x == 0) {
         part[blockIdx.x] = bb;
-        part[gridDim.x + blockIdx.x] = rz;
-        part[2 * gridDim.x + blockIdx.x] = rr;
+        part[A.nparts + blockIdx.x] = rz;
+        part[2 * A.nparts + blockIdx.x] = rr;
     }
 }
 
@@ -234,14 +271,17 @@ __global__ void k_cg_spmv(CG A, const double* __restrict__ p, double* __restrict
 {
     __shared__ double sh[33];
     if (flag[0]) return;
+    Grp<32> q;
+    const long nwarps = (long)gridDim.x * blockDim.x / 32;
     double ps = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+    for (long w = q.gid; w < A.n; w += nwarps) {
+        int i = (int)w;
         double si = 0;
         if (A.bcon[i] == 0) {
-            si = spmv_row(A, p, i);
-            ps += p[i] * si;
+            si = spmv_row_warp(A, q, p, i);
+            if (q.lane == 0) ps += p[i] * si;
         }
-        s[i] = si;
+        if (q.lane == 0) s[i] = si;
     }
     ps = block_sum(ps, sh);
     if (threadIdx.x == 0) part[blockIdx.x] = ps;
@@ -256,7 +296,7 @@ __global__ void k_cg_update(CG A, double* __restrict__ x, double* __restrict__ r
 {
     __shared__ double sh[33];
     if (flag[0]) return;
-    double ps = reduce_parts(part_ps, gridDim.x, sh);
+    double ps = reduce_parts(part_ps, A.nparts, sh);
     double alpha = scal[S_RZ] / ps;
     double rz = 0, rr = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
@@ -274,7 +314,7 @@ __global__ void k_cg_update(CG A, double* __restrict__ x, double* __restrict__ r
     rr = block_sum(rr, sh);
     if (threadIdx.x == 0) {
         part[blockIdx.x] = rz;
-        part[gridDim.x + blockIdx.x] = rr;
+        part[A.nparts + blockIdx.x] = rr;
     }
 }
 
@@ -287,8 +327,8 @@ __global__ void k_cg_direction(CG A, const double* __restrict__ zv, double* __re
 {
     __shared__ double sh[33];
     if (flag[0]) return;
-    double rz = reduce_parts(part, gridDim.x, sh);
-    double rr = reduce_parts(part + gridDim.x, gridDim.x, sh);
+    double rz = reduce_parts(part, A.nparts, sh);
+    double rr = reduce_parts(part + A.nparts, A.nparts, sh);
     double beta = rz / scal[S_RZ];
     int it = flag[1] + 1;
     bool done = (rr <= tol2 * scal[S_BB]) || it >= maxit || !(rr == rr);
@@ -338,37 +378,59 @@ int vmps_ppe(mps_ctx* c)
     cudaStream_t st = c->stream;
     const int n = c->n;
     const double *ax = c->x, *ay = c->y, *az = c->z, *nsrc = c->nd;
-    if (f.ppe_at_predicted) { ax = c->xs; ay = c->ys; az = c->zs; nsrc = c->nds; }
-    Asm A{f.re_l, c->lambda_l, c->n0_l, c->n0_s, f.rho1, f.dt, f.ktype, f.matopt, f.srcopt};
+    const double4* P4 = c->P4;
+    if (f.ppe_at_predicted) { ax = c->xs; ay = c->ys; az = c->zs; nsrc = c->nds; P4 = c->P4s; }
+    Asm A;
+    A.wk = make_wk(f.ktype, f.re_l);
+    A.cw = 2.0 * f.dim / c->lambda_l / c->n0_l / f.rho1;
+    A.cm = ((f.dim == 2) ? 3.0 * f.re_l : 2.0 * f.re_l) / c->n0_l / f.rho1;
+    A.reg = (1.00e-7) / f.dt / f.dt;
+    A.tiny2 = sqrt_cut(1.0e-15, false);
+    A.n0_s = c->n0_s;
+    A.dt = f.dt;
+    A.matopt = f.matopt;
+    A.srcopt = f.srcopt;
+    // CSR row offsets: exclusive scan of the Laplacian list lengths (each
+    // row's non-zeros are a subset of its list)
+    {
+        int r = vmps_scan(c, n, c->len_l, c->moff);
+        if (r != MPS_OK) return r;
+    }
+    const int wblocks = (int)(((long)n * 32 + kBlock - 1) / kBlock);
     if (f.dim == 3)
-        k_assemble<3><<<grid_blocks(n), kBlock, 0, st>>>(n, c->pitch, A, c->nbr_l, c->len_l, c->bcon,
-                                                     c->ptype, ax, ay, az, nsrc, f.warm_start,
-                                                     c->pnew, c->mcol, c->mval, c->mlen, c->diag,
-                                                     c->source);
+        k_assemble<3><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
+                                                  nsrc, f.warm_start, c->pnew, c->moff, c->mcol,
+                                                  c->mval, c->mlen, c->diag, c->source);
     else
-        k_assemble<2><<<grid_blocks(n), kBlock, 0, st>>>(n, c->pitch, A, c->nbr_l, c->len_l, c->bcon,
-                                                     c->ptype, ax, ay, az, nsrc, f.warm_start,
-                                                     c->pnew, c->mcol, c->mval, c->mlen, c->diag,
-                                                     c->source);
+        k_assemble<2><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
+                                                  nsrc, f.warm_start, c->pnew, c->moff, c->mcol,
+                                                  c->mval, c->mlen, c->diag, c->source);
     vmps_count_launch(1);
     if (f.srcopt) {
         // slot of particle id k: inv_id[k] (the sort's inv buffer is free here)
         k_invert<<<grid_blocks(n), kBlock, 0, st>>>(n, c->oid, c->inv);
         vmps_count_launch(1);
         if (f.dim == 3)
-            k_source_hs<3><<<1, 32, 0, st>>>(n, c->pitch, f.re_s, c->n0_s, f.dt, c->inv, c->nbr_s,
+            k_source_hs<3><<<1, 32, 0, st>>>(n, c->cap_s, f.re_s, c->n0_s, f.dt, c->inv, c->nbr_s,
                                              c->len_s, c->bcon, c->ptype, c->nds, ax, ay, az, c->us,
                                              c->vs, c->ws, c->source);
         else
-            k_source_hs<2><<<1, 32, 0, st>>>(n, c->pitch, f.re_s, c->n0_s, f.dt, c->inv, c->nbr_s,
+            k_source_hs<2><<<1, 32, 0, st>>>(n, c->cap_s, f.re_s, c->n0_s, f.dt, c->inv, c->nbr_s,
                                              c->len_s, c->bcon, c->ptype, c->nds, ax, ay, az, c->us,
                                              c->vs, c->ws, c->source);
         vmps_count_launch(1);
     }
-    CG G{c->mcol, c->mval, c->mlen, c->diag, c->bcon, c->pitch, n, f.solver == 1 ? 1 : 0};
-    int nblk = 0;
+    int nblk = 0, occ = 0;
     VMPS_CUDA(c, cudaDeviceGetAttribute(&nblk, cudaDevAttrMultiProcessorCount, c->device));
-    nblk *= 4;
+    VMPS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg_spmv, kRedThreads, 0));
+    nblk *= std::max(1, std::min(occ, 8));
+    // layout of cg_part: [0,3*nblk) start/update partials, [4*nblk,5*nblk) p.s
+    if ((size_t)5 * nblk > c->cg_part_cap) {
+        c->msg = "CG partial buffer too small for the launch grid";
+        return MPS_ERR_ARG;
+    }
+    CG G{c->mcol, c->mval, c->mlen, c->moff, c->diag, c->bcon, c->cap_l, n,
+         f.solver == 1 ? 1 : 0, nblk};
     double tol2 = f.cg_tol * f.cg_tol;
     k_cg_start<<<nblk, kRedThreads, 0, st>>>(G, c->source, c->pnew, c->cg_r, c->cg_z, c->cg_p,
                                              c->cg_part);

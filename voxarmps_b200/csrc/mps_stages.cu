@@ -1,10 +1,15 @@
-// mps_stages.cu -- explicit per-particle stages of one MPS step.
+// mps_stages.cu -- explicit per-particle stages of one MPS step (FP64).
 //
-// One thread per particle, neighbours visited in list order and accumulated
-// in FP64 with the reference's evaluation order (this unit is compiled with
-// -fmad=false), so each stage reproduces the oracle's sums.  Lists are the
-// slot-major ELL built by mps_neighbors.cu.  Reference routines are cited on
-// each kernel.
+// Each particle's neighbour row is walked by a group of lanes.  Every
+// support / cutoff decision the reference takes with sqrt() is taken here on
+// the squared distance against an exact threshold (same decision, see
+// sqrt_cut), and magnitudes use one rsqrt per pair instead of the
+// reference's sqrt and four divisions (functions.cu:32-89, 245-428), so each
+// term differs from the reference's by a few ulps at most.  Positions and
+// velocities are gathered as packed double4.  Lists are row-major (see
+// mps_internal.cuh): a group of G lanes walks one row, entries k = lane,
+// lane + G, ..., and the group's partial sums meet in a fixed butterfly.
+// Reference routines are cited on each kernel.
 #include "mps_internal.cuh"
 
 using namespace vmps;
@@ -14,40 +19,58 @@ namespace {
 struct Lists {
     const int* __restrict__ nbr;
     const int* __restrict__ len;
-    int pitch;
+    int cap;
 };
 
-__device__ __forceinline__ int nb(const Lists& L, int k, int i)
+__device__ __forceinline__ const int* row_of(const Lists& L, int i)
 {
-    return L.nbr[(size_t)k * L.pitch + i];
+    return L.nbr + (size_t)i * L.cap;
 }
 
 template <int DIM>
-__device__ __forceinline__ double dist_ij(const double* x, const double* y, const double* z, int i,
-                                          int j)
+__device__ __forceinline__ double d2of(const double4& a, const double4& b, double& dx, double& dy,
+                                       double& dz)
 {
-    double dz = DIM == 3 ? z[j] - z[i] : 0.0;
-    return sqrt(dist2<DIM>(x[j] - x[i], y[j] - y[i], dz));
+    dx = b.x - a.x;
+    dy = b.y - a.y;
+    dz = DIM == 3 ? b.z - a.z : 0.0;
+    return dist2<DIM>(dx, dy, dz);
+}
+
+// positions (x, y, z, ptype) when ptype != nullptr, else (a, b, c, 0)
+__global__ void k_pack(int n, const double* __restrict__ x, const double* __restrict__ y,
+                       const double* __restrict__ z, const int* __restrict__ ptype,
+                       double4* __restrict__ P4)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) P4[i] = make_double4(x[i], y[i], z[i], ptype ? (double)ptype[i] : 0.0);
 }
 
 // PNUM / PNUMSTAR (functions.cu:94-122, 157-179)
-template <int DIM>
-__global__ void k_pnd(int n, Lists L, const double* __restrict__ x, const double* __restrict__ y,
-                      const double* __restrict__ z, double re, int ktype, int correct,
+template <int DIM, int G>
+__global__ void k_pnd(int n, Lists L, const double4* __restrict__ P4, WK wk, int correct,
                       double ncorr, double* __restrict__ out, unsigned long long* dmax)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    Grp<G> q;
+    int i = (int)q.gid;
     if (i >= n) return;
-    double sum = 0.0;
+    double4 pi = P4[i];
+    const int* row = row_of(L, i);
     int len = L.len[i];
-    for (int k = 0; k < len; k++) {
-        int j = nb(L, k, i);
-        double d = dist_ij<DIM>(x, y, z, i, j);
-        if (i != j) sum = sum + kernel_w(d, ktype, DIM, re);
+    double sum = 0.0;
+    for (int k = q.lane; k < len; k += G) {
+        int j = row[k];
+        if (i == j) continue;
+        double dx, dy, dz;
+        double d2 = d2of<DIM>(pi, P4[j], dx, dy, dz);
+        sum += w_fast<DIM>(wk, d2, rsq(d2));
     }
-    if (correct && ktype != 2) sum = sum * ncorr;
-    out[i] = sum;
-    if (dmax && sum > 0.0) atomicMax(dmax, (unsigned long long)__double_as_longlong(sum));
+    sum = q.sum(sum);
+    if (q.lane == 0) {
+        if (correct && wk.ktype != 2) sum = sum * ncorr;
+        out[i] = sum;
+        if (dmax && sum > 0.0) atomicMax(dmax, (unsigned long long)__double_as_longlong(sum));
+    }
 }
 
 // BCON (functions.cu:433-445)
@@ -64,70 +87,76 @@ __global__ void k_bcon(int n, const int* __restrict__ ptype, const double* __res
 }
 
 // V_FRACTION (functions.cu:2580-2638)
-template <int DIM>
+template <int DIM, int G>
 __global__ void k_vfraction(int n, Lists L, const int* __restrict__ ptype,
-                            const double* __restrict__ x, const double* __restrict__ y,
-                            const double* __restrict__ z, double re, int ktype, int method,
+                            const double4* __restrict__ P4, WK wk, int method,
                             double* __restrict__ C)
 {
-    int I = blockIdx.x * blockDim.x + threadIdx.x;
+    Grp<G> q;
+    int I = (int)q.gid;
     if (I >= n) return;
     double sum1 = 0, sum2 = 0;
+    double4 pi = P4[I];
+    const int* row = row_of(L, I);
     int len = L.len[I];
-    for (int k = 0; k < len; k++) {
-        int J = nb(L, k, I);
+    for (int k = q.lane; k < len; k += G) {
+        int J = row[k];
         int pj = ptype[J];
-        if (method == 1) {
-            if (I != J && pj > 0) {
-                sum1 = sum1 + 1;
-                if (pj == 2) sum2 = sum2 + 1;
-            }
-        } else {
-            double d = dist_ij<DIM>(x, y, z, I, J);
-            if (I != J && pj > 0) {
-                double w = kernel_w(d, ktype, DIM, re);
-                sum1 = sum1 + w;
-                if (pj == 2) sum2 = sum2 + w;
-            }
+        if (I == J || pj <= 0) continue;
+        double w = 1.0;
+        if (method != 1) {
+            double dx, dy, dz;
+            double d2 = d2of<DIM>(pi, P4[J], dx, dy, dz);
+            w = w_fast<DIM>(wk, d2, rsq(d2));
         }
+        sum1 += w;
+        if (pj == 2) sum2 += w;
     }
-    double c = sum2 / sum1;
-    if (sum1 == 0) c = 0;
-    C[I] = c;
+    sum1 = q.sum(sum1);
+    sum2 = q.sum(sum2);
+    if (q.lane == 0) {
+        double c = sum2 / sum1;
+        if (sum1 == 0) c = 0;
+        C[I] = c;
+    }
 }
 
-// velocity-gradient sums of VISCOSITY / SPS (functions.cu:2096-2117, 1734-1756)
-template <int DIM>
-__device__ __forceinline__ void grad_sums(const Lists& L, int I, const double* x, const double* y,
-                                          const double* z, const double* un, const double* vn,
-                                          const double* wn, double re, int ktype, double mind,
-                                          double* s)
+// velocity-gradient sums of VISCOSITY / SPS (functions.cu:2096-2117, 1734-1756);
+// mind2 < 0: every pair (VISCOSITY); else pairs with d2 > mind2 (SPS d > coll/10).
+// Returns the group-reduced sums in every lane.
+template <int DIM, int G>
+__device__ __forceinline__ void grad_sums(const Grp<G>& q, const Lists& L, int I,
+                                          const double4* P4, const double* un, const double* vn,
+                                          const double* wn, const WK& wk, double mind2, double* s)
 {
     for (int k = 0; k < 9; k++) s[k] = 0.0;
+    const int* row = row_of(L, I);
     int len = L.len[I];
-    double xi = x[I], yi = y[I], zi = DIM == 3 ? z[I] : 0.0;
+    double4 pi = P4[I];
     double ui = un[I], vi = vn[I], wi = DIM == 3 ? wn[I] : 0.0;
-    for (int k = 0; k < len; k++) {
-        int j = nb(L, k, I);
-        double dx = x[j] - xi, dy = y[j] - yi, dz = DIM == 3 ? z[j] - zi : 0.0;
-        double d = sqrt(dist2<DIM>(dx, dy, dz));
-        if (I != j && (mind < 0 || d > mind)) {
-            double w = kernel_w(d, ktype, DIM, re);
-            double du = un[j] - ui, dv = vn[j] - vi;
-            s[0] = s[0] + du * dx * w / d / d;
-            s[1] = s[1] + dv * dy * w / d / d;
-            s[2] = s[2] + du * dy * w / d / d;
-            s[3] = s[3] + dv * dx * w / d / d;
-            if (DIM == 3) {
-                double dw = wn[j] - wi;
-                s[4] = s[4] + dw * dz * w / d / d;
-                s[5] = s[5] + du * dz * w / d / d;
-                s[6] = s[6] + dv * dz * w / d / d;
-                s[7] = s[7] + dw * dx * w / d / d;
-                s[8] = s[8] + dw * dy * w / d / d;
-            }
+    for (int k = q.lane; k < len; k += G) {
+        int j = row[k];
+        if (I == j) continue;
+        double dx, dy, dz;
+        double d2 = d2of<DIM>(pi, P4[j], dx, dy, dz);
+        if (!(mind2 < 0 || d2 > mind2)) continue;
+        double rD = rsq(d2);
+        double f = w_fast<DIM>(wk, d2, rD) * rD * rD;
+        double du = un[j] - ui, dv = vn[j] - vi;
+        s[0] += du * dx * f;
+        s[1] += dv * dy * f;
+        s[2] += du * dy * f;
+        s[3] += dv * dx * f;
+        if (DIM == 3) {
+            double dw = wn[j] - wi;
+            s[4] += dw * dz * f;
+            s[5] += du * dz * f;
+            s[6] += dv * dz * f;
+            s[7] += dw * dx * f;
+            s[8] += dw * dy * f;
         }
     }
+    for (int k = 0; k < (DIM == 3 ? 9 : 4); k++) s[k] = q.sum(s[k]);
 }
 
 // strain tensor S11 S12 S22 S13 S23 S33 (functions.cu:2118-2146)
@@ -150,35 +179,38 @@ __device__ __forceinline__ void strain(double n0, const double* s, double* S)
 }
 
 struct Phys {
-    double rho1, rho2, nu1, nu2, n0, meu0, n_pl, phi, cohes, cs, l0, mind;
-    int ktype, fluid2_type;
-    double re;
+    double rho1, rho2, nu1, nu2, n0, meu0, n_pl, phi, cohes, cs, l0, mind2;
+    int fluid2_type;
+    WK wk;
 };
 
 // VISCOSITY (functions.cu:2053-2184); reads C[i] where the reference reads
 // C[0] (identical whenever phi == 0)
-template <int DIM>
+template <int DIM, int G>
 __global__ void k_viscosity(int n, Lists L, Phys P, const int* __restrict__ ptype,
-                            const double* __restrict__ x, const double* __restrict__ y,
-                            const double* __restrict__ z, const double* __restrict__ un,
+                            const double4* __restrict__ P4, const double* __restrict__ un,
                             const double* __restrict__ vn, const double* __restrict__ wn,
                             const double* __restrict__ C, const double* __restrict__ phat,
                             double* __restrict__ meu)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    Grp<G> q;
+    int i = (int)q.gid;
     if (i >= n) return;
     int pt = ptype[i];
     if (P.fluid2_type == 0) {
-        if (pt <= 1) meu[i] = P.nu1 * P.rho1;
-        if (pt == 2) meu[i] = P.nu2 * P.rho2;
+        if (q.lane == 0) {
+            if (pt <= 1) meu[i] = P.nu1 * P.rho1;
+            if (pt == 2) meu[i] = P.nu2 * P.rho2;
+        }
         return;
     }
     if (pt == 1) {
-        meu[i] = P.nu1 * P.rho1;
+        if (q.lane == 0) meu[i] = P.nu1 * P.rho1;
         return;
     }
     double s[9], S[6];
-    grad_sums<DIM>(L, i, x, y, z, un, vn, wn, P.re, P.ktype, -1.0, s);
+    grad_sums<DIM, G>(q, L, i, P4, un, vn, wn, P.wk, -1.0, s);
+    if (q.lane != 0) return;
     strain<DIM>(P.n0, s, S);
     double phi = (C[i] - 0.25) * P.phi / (1 - 0.25);
     if (C[i] < 0.25) phi = 0;
@@ -196,54 +228,62 @@ __global__ void k_viscosity(int n, Lists L, Phys P, const int* __restrict__ ptyp
 }
 
 // SPS pass 1: strain tensor and eddy viscosity (functions.cu:1731-1790)
-template <int DIM>
+template <int DIM, int G>
 __global__ void k_sps1(int n, Lists L, Phys P, const int* __restrict__ ptype,
-                       const double* __restrict__ x, const double* __restrict__ y,
-                       const double* __restrict__ z, const double* __restrict__ un,
+                       const double4* __restrict__ P4, const double* __restrict__ un,
                        const double* __restrict__ vn, const double* __restrict__ wn,
                        double* __restrict__ S6, double* __restrict__ neut)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    Grp<G> q;
+    int i = (int)q.gid;
     if (i >= n || ptype[i] < 0) return;
     double s[9], S[6];
-    grad_sums<DIM>(L, i, x, y, z, un, vn, wn, P.re, P.ktype, P.mind, s);
+    grad_sums<DIM, G>(q, L, i, P4, un, vn, wn, P.wk, P.mind2, s);
+    if (q.lane != 0) return;
     strain<DIM>(P.n0, s, S);
     for (int c = 0; c < 6; c++) S6[(size_t)c * n + i] = S[c];
     double S11 = S[0], S12 = S[1], S22 = S[2], S13 = S[3], S23 = S[4], S33 = S[5];
     double Sm;
     if (DIM == 3)
-        Sm = pow(2 * S11 * S11, 0.5) + 2 * pow(2 * S12 * S12, 0.5) + pow(2 * S22 * S22, 0.5) +
-             pow(2 * S33 * S33, 0.5) + 2 * pow(2 * S13 * S13, 0.5) + 2 * pow(2 * S23 * S23, 0.5);
+        Sm = sqrt(2 * S11 * S11) + 2 * sqrt(2 * S12 * S12) + sqrt(2 * S22 * S22) +
+             sqrt(2 * S33 * S33) + 2 * sqrt(2 * S13 * S13) + 2 * sqrt(2 * S23 * S23);
     else
-        Sm = pow(2 * S11 * S11, 0.5) + 2 * pow(2 * S12 * S12, 0.5) + pow(2 * S22 * S22, 0.5);
+        Sm = sqrt(2 * S11 * S11) + 2 * sqrt(2 * S12 * S12) + sqrt(2 * S22 * S22);
     double cd = P.cs * P.l0;
     neut[i] = (cd * cd) * Sm;
 }
 
 // SPS pass 2: divergence of the SPS stress (functions.cu:1793-1830)
-template <int DIM>
+template <int DIM, int G>
 __global__ void k_sps2(int n, Lists L, Phys P, const int* __restrict__ ptype,
-                       const double* __restrict__ x, const double* __restrict__ y,
-                       const double* __restrict__ z, const double* __restrict__ S6,
+                       const double4* __restrict__ P4, const double* __restrict__ S6,
                        const double* __restrict__ neut, double* __restrict__ t1,
                        double* __restrict__ t2, double* __restrict__ t3)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    Grp<G> q;
+    int i = (int)q.gid;
     if (i >= n || ptype[i] < 0) return;
     double sum1 = 0, sum2 = 0, sum3 = 0;
+    const int* row = row_of(L, i);
     int len = L.len[i];
     double ni = neut[i];
-    for (int k = 0; k < len; k++) {
-        int j = nb(L, k, i);
-        double dx = x[j] - x[i], dy = y[j] - y[i], dz = DIM == 3 ? z[j] - z[i] : 0.0;
-        double d = sqrt(dist2<DIM>(dx, dy, dz));
-        if (i != j && d > P.mind) {
-            double w = kernel_w(d, P.ktype, DIM, P.re);
-            sum1 = sum1 + (neut[j] - ni) * dx * w / d / d;
-            sum2 = sum2 + (neut[j] - ni) * dy * w / d / d;
-            if (DIM == 3) sum3 = sum3 + (neut[j] - ni) * dz * w / d / d;
-        }
+    double4 pi = P4[i];
+    for (int k = q.lane; k < len; k += G) {
+        int j = row[k];
+        if (i == j) continue;
+        double dx, dy, dz;
+        double d2 = d2of<DIM>(pi, P4[j], dx, dy, dz);
+        if (!(d2 > P.mind2)) continue;
+        double rD = rsq(d2);
+        double f = (neut[j] - ni) * w_fast<DIM>(P.wk, d2, rD) * rD * rD;
+        sum1 += dx * f;
+        sum2 += dy * f;
+        if (DIM == 3) sum3 += dz * f;
     }
+    sum1 = q.sum(sum1);
+    sum2 = q.sum(sum2);
+    sum3 = q.sum(sum3);
+    if (q.lane != 0) return;
     double S11 = S6[i], S12 = S6[(size_t)n + i], S22 = S6[2 * (size_t)n + i];
     double S13 = S6[3 * (size_t)n + i], S23 = S6[4 * (size_t)n + i], S33 = S6[5 * (size_t)n + i];
     if (DIM == 3) {
@@ -257,91 +297,126 @@ __global__ void k_sps2(int n, Lists L, Phys P, const int* __restrict__ ptype,
 }
 
 struct PredArgs {
-    double re_s, n0_s, re_l, n0_l, lambda_l, dt, gx, gy, gz, relaxp, rho1, rho2;
-    int ktype;
+    WK ws, wl;
+    double n0_s, visc_coef, dt, gx, gy, gz, relaxp, rho1, rho2;
 };
 
-// PREDICTION (functions.cu:2283-2369): explicit pressure sums over the PND
-// list, viscous Laplacian over the Laplacian list.
-template <int DIM>
-__global__ void k_predict(int n, Lists Ls, Lists Ll, PredArgs A, const int* __restrict__ ptype,
-                          const double* __restrict__ meu, const double* __restrict__ x,
-                          const double* __restrict__ y, const double* __restrict__ z,
-                          const double* __restrict__ u, const double* __restrict__ v,
-                          const double* __restrict__ w, const double* __restrict__ pnew,
-                          const double* __restrict__ phat, const double* __restrict__ neut,
-                          const double* __restrict__ t1, const double* __restrict__ t2,
-                          const double* __restrict__ t3, const double* __restrict__ rho,
-                          double* __restrict__ xs, double* __restrict__ ys,
-                          double* __restrict__ zs, double* __restrict__ us,
-                          double* __restrict__ vs, double* __restrict__ ws)
+// PREDICTION (functions.cu:2283-2369), first part: the explicit pressure
+// sums over the PND list, scaled by (1-relaxp)*2*dt/(n0*rho) (fluid rows).
+template <int DIM, int G>
+__global__ void k_predict_p(int n, Lists Ls, PredArgs A, const double4* __restrict__ P4,
+                            const double* __restrict__ pnew, const double* __restrict__ phat,
+                            const double* __restrict__ rho, double* __restrict__ px,
+                            double* __restrict__ py, double* __restrict__ pz)
 {
-    int I = blockIdx.x * blockDim.x + threadIdx.x;
+    Grp<G> q;
+    int I = (int)q.gid;
     if (I >= n) return;
-    int pI = ptype[I];
+    double4 pi = P4[I];
+    if (pi.w <= 0) return;
+    double sum1 = 0, sum2 = 0, sum3 = 0;
+    double ph = phat[I];
+    const int* row = row_of(Ls, I);
+    int len = Ls.len[I];
+    for (int k = q.lane; k < len; k += G) {
+        int J = row[k];
+        if (I == J) continue;
+        double dx, dy, dz;
+        double d2 = d2of<DIM>(pi, P4[J], dx, dy, dz);
+        if (!(d2 > 0)) continue;
+        double rD = rsq(d2);
+        double f = (pnew[J] - ph) * w_fast<DIM>(A.ws, d2, rD) * rD * rD;
+        sum1 += dx * f;
+        sum2 += dy * f;
+        if (DIM == 3) sum3 += dz * f;
+    }
+    sum1 = q.sum(sum1);
+    sum2 = q.sum(sum2);
+    if (DIM == 3) sum3 = q.sum(sum3);
+    if (q.lane != 0) return;
+    double pc = (1 - A.relaxp) * (2.0 * A.dt / A.n0_s / rho[I]);
+    px[I] = pc * sum1;
+    py[I] = pc * sum2;
+    if (DIM == 3) pz[I] = pc * sum3;
+}
+
+// PREDICTION, second part: viscous Laplacian over the Laplacian list, one
+// warp per particle, then u* and x*.
+template <int DIM>
+__global__ void __launch_bounds__(256, 4)
+k_predict(int n, Lists Ll, PredArgs A, const double* __restrict__ meu,
+          const double4* __restrict__ P4, const double4* __restrict__ U4,
+          const double* __restrict__ px, const double* __restrict__ py,
+          const double* __restrict__ pz, const double* __restrict__ neut,
+          const double* __restrict__ t1, const double* __restrict__ t2,
+          const double* __restrict__ t3, double* __restrict__ xs, double* __restrict__ ys,
+          double* __restrict__ zs, double* __restrict__ us, double* __restrict__ vs,
+          double* __restrict__ ws, double4* __restrict__ P4s)
+{
+    Grp<32> q;
+    int I = (int)q.gid;
+    if (I >= n) return;
+    double4 pi = P4[I], ui4 = U4[I];
+    int pI = (int)pi.w;
     if (pI <= 0) {
-        xs[I] = x[I]; ys[I] = y[I]; us[I] = u[I]; vs[I] = v[I];
-        if (DIM == 3) { zs[I] = z[I]; ws[I] = w[I]; }
+        if (q.lane == 0) {
+            xs[I] = pi.x; ys[I] = pi.y; us[I] = ui4.x; vs[I] = ui4.y;
+            if (DIM == 3) { zs[I] = pi.z; ws[I] = ui4.z; }
+            P4s[I] = pi;
+        }
         return;
     }
-    double xi = x[I], yi = y[I], zi = DIM == 3 ? z[I] : 0.0;
-    double sum1 = 0, sum2 = 0, sum3 = 0, sum4 = 0, sum5 = 0, sum6 = 0, sum7 = 0, sum8 = 0, sum9 = 0;
-    double ph = phat[I];
-    int len = Ls.len[I];
-    for (int k = 0; k < len; k++) {
-        int J = nb(Ls, k, I);
-        double dx = x[J] - xi, dy = y[J] - yi, dz = DIM == 3 ? z[J] - zi : 0.0;
-        double D = sqrt(dist2<DIM>(dx, dy, dz));
-        if (I != J && D > 0) {
-            double W = kernel_w(D, A.ktype, DIM, A.re_s);
-            double pp = pnew[J] - ph;
-            sum1 = sum1 + pp * dx * W / D / D;
-            sum2 = sum2 + pp * dy * W / D / D;
-            if (DIM == 3) sum3 = sum3 + pp * dz * W / D / D;
+    double sum4 = 0, sum5 = 0, sum6 = 0, sum7 = 0, sum8 = 0, sum9 = 0;
+    double mI = meu[I];
+    double rhoI = (pI == 1) ? A.rho1 : A.rho2;
+    double neu_same = mI / rhoI;
+    const int* row = row_of(Ll, I);
+    int len = Ll.len[I];
+    for (int k = q.lane; k < len; k += 32) {
+        int J = row[k];
+        if (I == J) continue;
+        double4 pj = P4[J];
+        double dx, dy, dz;
+        double d2 = d2of<DIM>(pi, pj, dx, dy, dz);
+        if (!(d2 > 0)) continue;
+        double W = w_fast<DIM>(A.wl, d2, rsq(d2));
+        double NEU = neu_same;
+        if ((int)pj.w != pI) {
+            double mJ = meu[J];
+            NEU = 2 * mI * mJ / (mI + mJ) / rhoI;
+        }
+        double4 uj = U4[J];
+        double du = W * (uj.x - ui4.x), dv = W * (uj.y - ui4.y);
+        sum4 += du * NEU;
+        sum5 += dv * NEU;
+        sum7 += du;
+        sum8 += dv;
+        if (DIM == 3) {
+            double dw = W * (uj.z - ui4.z);
+            sum6 += dw * NEU;
+            sum9 += dw;
         }
     }
-    double mI = meu[I], uI = u[I], vI = v[I], wI = DIM == 3 ? w[I] : 0.0;
-    len = Ll.len[I];
-    for (int k = 0; k < len; k++) {
-        int J = nb(Ll, k, I);
-        double dx = x[J] - xi, dy = y[J] - yi, dz = DIM == 3 ? z[J] - zi : 0.0;
-        double D = sqrt(dist2<DIM>(dx, dy, dz));
-        if (I != J && D > 0) {
-            double NEU;
-            if (pI == ptype[J]) {
-                NEU = (pI == 1) ? mI / A.rho1 : mI / A.rho2;
-            } else {
-                double mJ = meu[J];
-                NEU = (pI == 1) ? 2 * mI * mJ / (mI + mJ) / A.rho1 : 2 * mI * mJ / (mI + mJ) / A.rho2;
-            }
-            double W = kernel_w(D, A.ktype, DIM, A.re_l);
-            double du = u[J] - uI, dv = v[J] - vI;
-            sum4 = sum4 + W * du * NEU;
-            sum5 = sum5 + W * dv * NEU;
-            sum7 = sum7 + W * du;
-            sum8 = sum8 + W * dv;
-            if (DIM == 3) {
-                double dw = w[J] - wI;
-                sum6 = sum6 + W * dw * NEU;
-                sum9 = sum9 + W * dw;
-            }
-        }
-    }
-    double DT = A.dt, rp = 1 - A.relaxp, nt = neut[I], r = rho[I];
-    double uS = uI + A.gx * DT + 4 * DT * (sum4 + nt * sum7) / (A.lambda_l * A.n0_l) + DT * t1[I] -
-                rp * (2.0 * DT / A.n0_s / r) * sum1;
-    double vS = vI + A.gy * DT + 4 * DT * (sum5 + nt * sum8) / (A.lambda_l * A.n0_l) + DT * t2[I] -
-                rp * (2.0 * DT / A.n0_s / r) * sum2;
+    sum4 = q.sum(sum4); sum5 = q.sum(sum5); sum7 = q.sum(sum7); sum8 = q.sum(sum8);
+    if (DIM == 3) { sum6 = q.sum(sum6); sum9 = q.sum(sum9); }
+    if (q.lane != 0) return;
+    double DT = A.dt, nt = neut[I];
+    double uS = ui4.x + A.gx * DT + A.visc_coef * (sum4 + nt * sum7) + DT * t1[I] - px[I];
+    double vS = ui4.y + A.gy * DT + A.visc_coef * (sum5 + nt * sum8) + DT * t2[I] - py[I];
+    double4 o = pi;
+    o.x = pi.x + DT * uS;
+    o.y = pi.y + DT * vS;
     us[I] = uS;
     vs[I] = vS;
-    xs[I] = xi + DT * uS;
-    ys[I] = yi + DT * vS;
+    xs[I] = o.x;
+    ys[I] = o.y;
     if (DIM == 3) {
-        double wS = wI + A.gz * DT + 4 * DT * (sum6 + nt * sum9) / (A.lambda_l * A.n0_l) +
-                    DT * t3[I] - rp * (2.0 * DT / A.n0_s / r) * sum3;
+        double wS = ui4.z + A.gz * DT + A.visc_coef * (sum6 + nt * sum9) + DT * t3[I] - pz[I];
         ws[I] = wS;
-        zs[I] = zi + DT * wS;
+        o.z = pi.z + DT * wS;
+        zs[I] = o.z;
     }
+    P4s[I] = o;
 }
 
 // weakly compressible EOS (functions.cu:2467-2500)
@@ -362,63 +437,78 @@ __global__ void k_pressure_wc(int n, const int* __restrict__ ptype, const double
     pnew[I] = p;
 }
 
-// PHATCALC (functions.cu:207-224)
-__global__ void k_phat(int n, Lists L, const double* __restrict__ pnew, double* __restrict__ phat)
+// PHATCALC (functions.cu:207-224); also packs (pnew, phat) for the gradient
+template <int G>
+__global__ void k_phat(int n, Lists L, const double* __restrict__ pnew, double* __restrict__ phat,
+                       double2* __restrict__ PH)
 {
-    int I = blockIdx.x * blockDim.x + threadIdx.x;
+    Grp<G> q;
+    int I = (int)q.gid;
     if (I >= n) return;
     double mn = 999999999999999;
+    const int* row = row_of(L, I);
     int len = L.len[I];
-    for (int k = 0; k < len; k++) {
-        double pj = pnew[nb(L, k, I)];
+    for (int k = q.lane; k < len; k += G) {
+        double pj = pnew[row[k]];
         if (pj < mn) mn = pj;
     }
-    phat[I] = mn;
+    mn = q.min(mn);
+    if (q.lane == 0) {
+        phat[I] = mn;
+        PH[I] = make_double2(pnew[I], mn);
+    }
 }
 
 struct GradArgs {
-    double re, n0, dt, relaxp, vmax;
-    int ktype, kh;
+    WK wk;
+    double coef, vmax;
+    int kh;
 };
 
 // PRESSGRAD (functions.cu:245-355), CPU semantics (p^_i + p^_j)
-template <int DIM>
+template <int DIM, int G>
 __global__ void k_pressgrad(int n, Lists L, GradArgs A, const int* __restrict__ ptype,
-                            const double* __restrict__ pnew, const double* __restrict__ phat,
-                            const double* __restrict__ xs, const double* __restrict__ ys,
-                            const double* __restrict__ zs, const double* __restrict__ rho,
-                            const double* __restrict__ us, const double* __restrict__ vs,
-                            const double* __restrict__ ws, double* __restrict__ un,
-                            double* __restrict__ vn, double* __restrict__ wn)
+                            const double2* __restrict__ PH, const double4* __restrict__ P4s,
+                            const double* __restrict__ rho, const double* __restrict__ us,
+                            const double* __restrict__ vs, const double* __restrict__ ws,
+                            double* __restrict__ un, double* __restrict__ vn,
+                            double* __restrict__ wn)
 {
-    int I = blockIdx.x * blockDim.x + threadIdx.x;
+    Grp<G> q;
+    int I = (int)q.gid;
     if (I >= n || ptype[I] <= 0) return;
     double sum1 = 0, sum2 = 0, sum3 = 0;
-    double xi = xs[I], yi = ys[I], zi = DIM == 3 ? zs[I] : 0.0;
-    double pi = pnew[I], phi = phat[I];
+    double4 pi = P4s[I];
+    double2 phI = PH[I];
+    const int* row = row_of(L, I);
     int len = L.len[I];
-    for (int k = 0; k < len; k++) {
-        int J = nb(L, k, I);
-        double dx = xs[J] - xi, dy = ys[J] - yi, dz = DIM == 3 ? zs[J] - zi : 0.0;
-        double D = sqrt(dist2<DIM>(dx, dy, dz));
-        if (I != J) {
-            double w = kernel_w(D, A.ktype, DIM, A.re);
-            double pp = (A.kh == 1) ? pnew[J] + pi - (phi + phat[J]) : pnew[J] - phi;
-            sum1 = sum1 + pp * dx * w / D / D;
-            sum2 = sum2 + pp * dy * w / D / D;
-            if (DIM == 3) sum3 = sum3 + pp * dz * w / D / D;
-        }
+    for (int k = q.lane; k < len; k += G) {
+        int J = row[k];
+        if (I == J) continue;
+        double dx, dy, dz;
+        double d2 = d2of<DIM>(pi, P4s[J], dx, dy, dz);
+        double rD = rsq(d2);
+        double2 phJ = PH[J];
+        double pp = (A.kh == 1) ? phJ.x + phI.x - (phI.y + phJ.y) : phJ.x - phI.y;
+        double f = pp * w_fast<DIM>(A.wk, d2, rD) * rD * rD;
+        sum1 += dx * f;
+        sum2 += dy * f;
+        if (DIM == 3) sum3 += dz * f;
     }
-    double Rho = rho[I], DT = A.dt, VMAX = A.vmax, coeff = 2.0;
-    double uN = us[I] - A.relaxp * (2.0 * DT / A.n0 / Rho) * sum1;
-    double vN = vs[I] - A.relaxp * (2.0 * DT / A.n0 / Rho) * sum2;
+    sum1 = q.sum(sum1);
+    sum2 = q.sum(sum2);
+    if (DIM == 3) sum3 = q.sum(sum3);
+    if (q.lane != 0) return;
+    double c = A.coef / rho[I], VMAX = A.vmax, coeff = 2.0;
+    double uN = us[I] - c * sum1;
+    double vN = vs[I] - c * sum2;
     if (fabs(uN) > coeff * VMAX) uN = VMAX;
     if (vN > coeff * VMAX) vN = coeff * VMAX;
     if (vN < -coeff * VMAX) vN = -coeff * VMAX;
     un[I] = uN;
     vn[I] = vN;
     if (DIM == 3) {
-        double wN = ws[I] - A.relaxp * (2.0 * DT / A.n0 / Rho) * sum3;
+        double wN = ws[I] - c * sum3;
         if (fabs(wN) > coeff * VMAX) wN = VMAX;
         wn[I] = wN;
     }
@@ -433,7 +523,7 @@ template <int DIM>
 __global__ void k_integrate(int n, Box B, const int* __restrict__ ptype, double* __restrict__ x,
                             double* __restrict__ y, double* __restrict__ z,
                             double* __restrict__ un, double* __restrict__ vn,
-                            double* __restrict__ wn)
+                            double* __restrict__ wn, double4* __restrict__ P4)
 {
     int I = blockIdx.x * blockDim.x + threadIdx.x;
     if (I >= n || ptype[I] <= 0) return;
@@ -444,54 +534,60 @@ __global__ void k_integrate(int n, Box B, const int* __restrict__ ptype, double*
     if (yi > B.ymax - DL * 3.0) { vi = -fabs(vi) * CC; yi = B.ymax - DL * 3.0; }
     if (xi < B.xmin + DL * 3.0) { ui = fabs(ui) * CC; xi = B.xmin + DL * 3.0; }
     if (xi > B.xmax - DL * 3.0) { ui = -fabs(ui) * CC; xi = B.xmax - DL * 3.0; }
+    double zi = 0.0;
     if (DIM == 3) {
-        double zi = z[I] + wn[I] * DT, wi = wn[I];
+        double wi = wn[I];
+        zi = z[I] + wn[I] * DT;
         if (zi < B.zmin + DL * 3.0) { wi = fabs(wi) * CC; zi = B.zmin + DL * 3.0; }
         if (zi > B.zmax - DL * 3.0) { wi = -fabs(wi) * CC; zi = B.zmax - DL * 3.0; }
         z[I] = zi;
         wn[I] = wi;
     }
     x[I] = xi; y[I] = yi; un[I] = ui; vn[I] = vi;
+    P4[I] = make_double4(xi, yi, zi, P4[I].w);
 }
 
 struct CollArgs {
-    double coll, cc, dt, rho1, rho2;
+    double coll2, cc, dt, rho1, rho2;
 };
 
 // COLLISION2 (functions.cu:1523-1601) in its order-independent form: each
 // fluid particle gathers the impulse of every approaching pair (d < coll)
 // from the pre-collision state.  Writes the new state to the *o arrays.
-template <int DIM>
+template <int DIM, int G>
 __global__ void k_collision(int n, Lists L, CollArgs A, const int* __restrict__ ptype,
-                            const double* __restrict__ x, const double* __restrict__ y,
-                            const double* __restrict__ z, const double* __restrict__ un,
+                            const double4* __restrict__ P4, const double* __restrict__ un,
                             const double* __restrict__ vn, const double* __restrict__ wn,
                             double* __restrict__ xo, double* __restrict__ yo,
                             double* __restrict__ zo, double* __restrict__ uo,
-                            double* __restrict__ vo, double* __restrict__ wo)
+                            double* __restrict__ vo, double* __restrict__ wo,
+                            double4* __restrict__ P4o)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    Grp<G> q;
+    int i = (int)q.gid;
     if (i >= n) return;
-    double xi = x[i], yi = y[i], zi = DIM == 3 ? z[i] : 0.0;
+    double4 pi = P4[i];
     double ui = un[i], vi = vn[i], wi = DIM == 3 ? wn[i] : 0.0;
-    int pi = ptype[i];
+    int pti = ptype[i];
     double du = 0, dv = 0, dw = 0, ddx = 0, ddy = 0, ddz = 0;
-    if (pi > 0) {
-        double m1 = (pi == 1) ? A.rho1 : A.rho2;
+    if (pti > 0) {
+        double m1 = (pti == 1) ? A.rho1 : A.rho2;
+        const int* row = row_of(L, i);
         int len = L.len[i];
-        for (int k = 0; k < len; k++) {
-            int j = nb(L, k, i);
-            double ex = x[j] - xi, ey = y[j] - yi, ez = DIM == 3 ? z[j] - zi : 0.0;
-            double d = sqrt(dist2<DIM>(ex, ey, ez));
-            if (i == j || !(d < A.coll)) continue;
+        for (int k = q.lane; k < len; k += G) {
+            int j = row[k];
+            if (i == j) continue;
+            double ex, ey, ez;
+            double d2 = d2of<DIM>(pi, P4[j], ex, ey, ez);
+            if (!(d2 < A.coll2)) continue;
+            double d = sqrt(d2);
             double m2 = (ptype[j] == 1) ? A.rho1 : A.rho2;
             double ug = (m1 * ui + m2 * un[j]) / (m1 + m2);
             double vg = (m1 * vi + m2 * vn[j]) / (m1 + m2);
             double ur = m1 * (ui - ug), vr = m1 * (vi - vg), vabs;
-            double wr = 0;
             if (DIM == 3) {
                 double wg = (m1 * wi + m2 * wn[j]) / (m1 + m2);
-                wr = m1 * (wi - wg);
+                double wr = m1 * (wi - wg);
                 vabs = (ur * ex + vr * ey + wr * ez) / d;
             } else {
                 vabs = (ur * ex + vr * ey) / d;
@@ -506,9 +602,14 @@ __global__ void k_collision(int n, Lists L, CollArgs A, const int* __restrict__ 
                 dw -= wm / m1; ddz -= A.dt * wm / m1;
             }
         }
+        du = q.sum(du); dv = q.sum(dv); ddx = q.sum(ddx); ddy = q.sum(ddy);
+        if (DIM == 3) { dw = q.sum(dw); ddz = q.sum(ddz); }
     }
-    xo[i] = xi + ddx; yo[i] = yi + ddy; uo[i] = ui + du; vo[i] = vi + dv;
-    if (DIM == 3) { zo[i] = zi + ddz; wo[i] = wi + dw; }
+    if (q.lane != 0) return;
+    double4 o = make_double4(pi.x + ddx, pi.y + ddy, DIM == 3 ? pi.z + ddz : pi.z, pi.w);
+    xo[i] = o.x; yo[i] = o.y; uo[i] = ui + du; vo[i] = vi + dv;
+    if (DIM == 3) { zo[i] = o.z; wo[i] = wi + dw; }
+    P4o[i] = o;
 }
 
 // PREPDATA (functions.cu:2688-2746): roll state, flag ERROR#1 / ERROR#2
@@ -542,7 +643,7 @@ __global__ void k_commit(int n, Box B, const int* __restrict__ ptype,
 Lists lists(mps_ctx* c, int which)
 {
     Lists L;
-    L.pitch = c->pitch;
+    L.cap = which == 0 ? c->cap_l : c->cap_s;
     L.nbr = which == 0 ? c->nbr_l : c->nbr_s;
     L.len = which == 0 ? c->len_l : c->len_s;
     return L;
@@ -554,7 +655,9 @@ Phys phys(mps_ctx* c)
     const mps_config& f = c->cfg;
     P.rho1 = f.rho1; P.rho2 = f.rho2; P.nu1 = f.nu1; P.nu2 = f.nu2; P.n0 = c->n0_s;
     P.meu0 = f.meu0; P.n_pl = f.n_pl; P.phi = f.phi; P.cohes = f.cohes; P.cs = f.cs; P.l0 = f.l0;
-    P.mind = f.coll / 10; P.ktype = f.ktype; P.fluid2_type = f.fluid2_type; P.re = f.re_s;
+    P.mind2 = sqrt_cut(f.coll / 10, false);
+    P.fluid2_type = f.fluid2_type;
+    P.wk = make_wk(f.ktype, f.re_s);
     return P;
 }
 
@@ -572,15 +675,55 @@ Box box(mps_ctx* c)
         vmps_count_launch(1);                                                             \
     } while (0)
 
+inline int group_blocks(long n, int G) { return (int)((n * G + kBlock - 1) / kBlock); }
+
+// G lanes per PND-radius row (SmallG), or a whole warp (G = 32)
+#define LAUNCH_SMALL(kern, ...)                                                           \
+    do {                                                                                  \
+        if (c->cfg.dim == 3)                                                              \
+            kern<3, SmallG<3>::G><<<group_blocks(c->n, SmallG<3>::G), kBlock, 0, c->stream>>>( \
+                __VA_ARGS__);                                                             \
+        else                                                                              \
+            kern<2, SmallG<2>::G><<<group_blocks(c->n, SmallG<2>::G), kBlock, 0, c->stream>>>( \
+                __VA_ARGS__);                                                             \
+        vmps_count_launch(1);                                                             \
+    } while (0)
+#define LAUNCH_WARP(kern, ...)                                                            \
+    do {                                                                                  \
+        if (c->cfg.dim == 3)                                                              \
+            kern<3><<<group_blocks(c->n, 32), kBlock, 0, c->stream>>>(__VA_ARGS__);       \
+        else                                                                              \
+            kern<2><<<group_blocks(c->n, 32), kBlock, 0, c->stream>>>(__VA_ARGS__);       \
+        vmps_count_launch(1);                                                             \
+    } while (0)
+
 }  // namespace
+
+int vmps_pack(mps_ctx* c)
+{
+    k_pack<<<grid_blocks(c->n), kBlock, 0, c->stream>>>(c->n, c->x, c->y, c->z, c->ptype, c->P4);
+    k_pack<<<grid_blocks(c->n), kBlock, 0, c->stream>>>(c->n, c->u, c->v, c->w, nullptr, c->U4);
+    vmps_count_launch(2);
+    VMPS_CUDA(c, cudaGetLastError());
+    return MPS_OK;
+}
 
 int vmps_pnd(mps_ctx* c, int at_star, int correct, int which, double* out)
 {
-    const double *x = at_star ? c->xs : c->x, *y = at_star ? c->ys : c->y,
-                 *z = at_star ? c->zs : c->z;
     double re = which == 0 ? c->cfg.re_l : c->cfg.re_s;
-    LAUNCH_DIM(k_pnd, c->n, lists(c, which), x, y, z, re, c->cfg.ktype, correct,
-               c->cfg.ncorrection, out, c->d_max);
+    const double4* P = at_star ? c->P4s : c->P4;
+    WK wk = make_wk(c->cfg.ktype, re);
+    if (which == 0) {
+        if (c->cfg.dim == 3)
+            k_pnd<3, 32><<<group_blocks(c->n, 32), kBlock, 0, c->stream>>>(
+                c->n, lists(c, 0), P, wk, correct, c->cfg.ncorrection, out, c->d_max);
+        else
+            k_pnd<2, 32><<<group_blocks(c->n, 32), kBlock, 0, c->stream>>>(
+                c->n, lists(c, 0), P, wk, correct, c->cfg.ncorrection, out, c->d_max);
+        vmps_count_launch(1);
+    } else {
+        LAUNCH_SMALL(k_pnd, c->n, lists(c, 1), P, wk, correct, c->cfg.ncorrection, out, c->d_max);
+    }
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
 }
@@ -596,16 +739,16 @@ int vmps_bcon(mps_ctx* c)
 
 int vmps_vfraction(mps_ctx* c)
 {
-    LAUNCH_DIM(k_vfraction, c->n, lists(c, 1), c->ptype, c->x, c->y, c->z, c->cfg.re_s,
-               c->cfg.ktype, c->cfg.fraction_method, c->C);
+    LAUNCH_SMALL(k_vfraction, c->n, lists(c, 1), c->ptype, c->P4, make_wk(c->cfg.ktype, c->cfg.re_s),
+               c->cfg.fraction_method, c->C);
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
 }
 
 int vmps_viscosity(mps_ctx* c)
 {
-    LAUNCH_DIM(k_viscosity, c->n, lists(c, 1), phys(c), c->ptype, c->x, c->y, c->z, c->un, c->vn,
-               c->wn, c->C, c->phat, c->meu);
+    LAUNCH_SMALL(k_viscosity, c->n, lists(c, 1), phys(c), c->ptype, c->P4, c->un, c->vn, c->wn, c->C,
+               c->phat, c->meu);
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
 }
@@ -613,10 +756,8 @@ int vmps_viscosity(mps_ctx* c)
 int vmps_sps(mps_ctx* c)
 {
     Phys P = phys(c);
-    LAUNCH_DIM(k_sps1, c->n, lists(c, 1), P, c->ptype, c->x, c->y, c->z, c->un, c->vn, c->wn,
-               c->S6, c->neut);
-    LAUNCH_DIM(k_sps2, c->n, lists(c, 1), P, c->ptype, c->x, c->y, c->z, c->S6, c->neut, c->t1,
-               c->t2, c->t3);
+    LAUNCH_SMALL(k_sps1, c->n, lists(c, 1), P, c->ptype, c->P4, c->un, c->vn, c->wn, c->S6, c->neut);
+    LAUNCH_SMALL(k_sps2, c->n, lists(c, 1), P, c->ptype, c->P4, c->S6, c->neut, c->t1, c->t2, c->t3);
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
 }
@@ -624,11 +765,20 @@ int vmps_sps(mps_ctx* c)
 int vmps_predict(mps_ctx* c)
 {
     const mps_config& f = c->cfg;
-    PredArgs A{f.re_s, c->n0_s, f.re_l, c->n0_l, c->lambda_l, f.dt, f.gx, f.gy, f.gz, f.relaxp,
-               f.rho1, f.rho2, f.ktype};
-    LAUNCH_DIM(k_predict, c->n, lists(c, 1), lists(c, 0), A, c->ptype, c->meu, c->x, c->y, c->z,
-               c->u, c->v, c->w, c->pnew, c->phat, c->neut, c->t1, c->t2, c->t3, c->rho, c->xs,
-               c->ys, c->zs, c->us, c->vs, c->ws);
+    PredArgs A;
+    A.ws = make_wk(f.ktype, f.re_s);
+    A.wl = make_wk(f.ktype, f.re_l);
+    A.n0_s = c->n0_s;
+    // 4*DT/(lambda*n0) of the viscous term (functions.cu:2361; "4" is the
+    // reference's 2*d with d = 2, kept in 3D as well)
+    A.visc_coef = 4 * f.dt / (c->lambda_l * c->n0_l);
+    A.dt = f.dt; A.gx = f.gx; A.gy = f.gy; A.gz = f.gz; A.relaxp = f.relaxp;
+    A.rho1 = f.rho1; A.rho2 = f.rho2;
+    LAUNCH_SMALL(k_predict_p, c->n, lists(c, 1), A, c->P4, c->pnew, c->phat, c->rho, c->pres_x,
+                 c->pres_y, c->pres_z);
+    LAUNCH_WARP(k_predict, c->n, lists(c, 0), A, c->meu, c->P4, c->U4, c->pres_x, c->pres_y,
+                c->pres_z, c->neut, c->t1, c->t2, c->t3, c->xs, c->ys, c->zs, c->us, c->vs, c->ws,
+                c->P4s);
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
 }
@@ -646,7 +796,12 @@ int vmps_pressure_wc(mps_ctx* c)
 
 int vmps_phat(mps_ctx* c)
 {
-    k_phat<<<grid_blocks(c->n), kBlock, 0, c->stream>>>(c->n, lists(c, 1), c->pnew, c->phat);
+    if (c->cfg.dim == 3)
+        k_phat<SmallG<3>::G><<<group_blocks(c->n, SmallG<3>::G), kBlock, 0, c->stream>>>(
+            c->n, lists(c, 1), c->pnew, c->phat, c->PH);
+    else
+        k_phat<SmallG<2>::G><<<group_blocks(c->n, SmallG<2>::G), kBlock, 0, c->stream>>>(
+            c->n, lists(c, 1), c->pnew, c->phat, c->PH);
     vmps_count_launch(1);
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
@@ -655,16 +810,20 @@ int vmps_phat(mps_ctx* c)
 int vmps_pressgrad(mps_ctx* c)
 {
     const mps_config& f = c->cfg;
-    GradArgs A{f.re_s, c->n0_s, f.dt, f.relaxp, f.vmax, f.ktype, f.kh};
-    LAUNCH_DIM(k_pressgrad, c->n, lists(c, 1), A, c->ptype, c->pnew, c->phat, c->xs, c->ys, c->zs,
-               c->rho, c->us, c->vs, c->ws, c->un, c->vn, c->wn);
+    GradArgs A;
+    A.wk = make_wk(f.ktype, f.re_s);
+    A.coef = f.relaxp * (2.0 * f.dt / c->n0_s);
+    A.vmax = f.vmax;
+    A.kh = f.kh;
+    LAUNCH_SMALL(k_pressgrad, c->n, lists(c, 1), A, c->ptype, c->PH, c->P4s, c->rho, c->us, c->vs,
+               c->ws, c->un, c->vn, c->wn);
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
 }
 
 int vmps_integrate(mps_ctx* c)
 {
-    LAUNCH_DIM(k_integrate, c->n, box(c), c->ptype, c->x, c->y, c->z, c->un, c->vn, c->wn);
+    LAUNCH_DIM(k_integrate, c->n, box(c), c->ptype, c->x, c->y, c->z, c->un, c->vn, c->wn, c->P4);
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
 }
@@ -672,15 +831,16 @@ int vmps_integrate(mps_ctx* c)
 int vmps_collision(mps_ctx* c)
 {
     const mps_config& f = c->cfg;
-    CollArgs A{f.coll, f.cc, f.dt, f.rho1, f.rho2};
+    CollArgs A{sqrt_cut(f.coll, true), f.cc, f.dt, f.rho1, f.rho2};
     // the new state goes to the *c buffers, which then swap roles with it
-    LAUNCH_DIM(k_collision, c->n, lists(c, 1), A, c->ptype, c->x, c->y, c->z, c->un, c->vn, c->wn,
-               c->xc, c->yc, c->zc, c->uc, c->vc, c->wc);
+    LAUNCH_SMALL(k_collision, c->n, lists(c, 1), A, c->ptype, c->P4, c->un, c->vn, c->wn, c->xc,
+               c->yc, c->zc, c->uc, c->vc, c->wc, c->P4c);
     VMPS_CUDA(c, cudaGetLastError());
     std::swap(c->x, c->xc);
     std::swap(c->y, c->yc);
     std::swap(c->un, c->uc);
     std::swap(c->vn, c->vc);
+    std::swap(c->P4, c->P4c);
     if (c->cfg.dim == 3) {
         std::swap(c->z, c->zc);
         std::swap(c->wn, c->wc);
