@@ -151,6 +151,24 @@ int mps_write_vtu(mps_ctx* ctx, const char* path, int fluid_only);
 /* Device stream the context launches on (cudaStream_t as void*). */
 void* mps_stream(mps_ctx* ctx);
 
+/* Allocation-free binning: the 1-based cell number of every particle and
+ * the particles in cell order (ascending index inside a cell), for the grid
+ * of support radius re over the box in cfg -- the first half of NEIGHBOR --
+ * written to caller-owned device buffers.  For callers that may not
+ * allocate device memory (an application that owns the whole device heap
+ * through its own pool, or a loop that forbids allocation after start-up).
+ * It has no counterpart in the reference.  x, y, z (z unused in 2D): device
+ * positions; cell, perm: device outputs of n ints; out_of_grid: device word
+ * set non-zero when a particle lies outside the grid; stream: cudaStream_t
+ * or NULL.  Limits: n <= 262,144 particles and at most 262,142 cells;
+ * larger inputs return MPS_ERR_ARG.  Scratch is a fixed static device area
+ * shared by all calls (calls that overlap on the GPU race); the first call
+ * on each device looks its address up and should come before any stream
+ * capture.  Asynchronous on stream. */
+int mps_cell_order_noalloc(const mps_config* cfg, double re, int n, const double* x,
+                           const double* y, const double* z, int* cell, int* perm,
+                           unsigned int* out_of_grid, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -44,6 +44,7 @@ EXPORTS = [
     "mps_integrate", "mps_collision", "mps_commit", "mps_step", "mps_run", "mps_download",
     "mps_download_lists", "mps_get_scalar", "mps_get_error", "mps_last_message",
     "mps_write_vtu", "mps_stream", "mps_set_state", "mps_get_state", "mps_set_profile",
+    "mps_cell_order_noalloc",
 ]
 
 _LIB = None
@@ -88,6 +89,8 @@ def load_library(path: str = LIB_PATH):
     lib.mps_set_state.argtypes = [P, P, P, P, P, P, P, P]
     lib.mps_get_state.argtypes = [P, P, P, P, P, P, P, P]
     lib.mps_set_profile.argtypes = [P, C.c_int]
+    lib.mps_cell_order_noalloc.argtypes = [C.POINTER(MpsConfig), C.c_double, C.c_int, P, P, P,
+                                           P, P, P, P]
     _LIB = lib
     return lib
 
