@@ -215,6 +215,7 @@ int allocate(mps_ctx* c)
     TRY(dalloc(c, &c->P4s, P));
     TRY(dalloc(c, &c->P4c, P));
     TRY(dalloc(c, &c->U4, P));
+    TRY(dalloc(c, &c->P4f, P));
     TRY(dalloc(c, &c->PH, P));
     TRY(dalloc(c, &c->cnt_l, (size_t)c->gl.tnc + 2));
     TRY(dalloc(c, &c->cst_l, (size_t)c->gl.tnc + 2));
@@ -351,6 +352,19 @@ int mps_upload(mps_ctx* c, int n, const double* x, const double* y, const double
     if ((long long)c->gl.tnc > (1LL << 30) || (long long)c->gs.tnc > (1LL << 30)) {
         c->msg = "cell grid too large";
         return MPS_ERR_ARG;
+    }
+    // FP32 screening bound: coordinates stored relative to the box minimum
+    // carry an absolute error e <= extent * 2^-24 each, a difference of two
+    // at most 2e + |dx| 2^-24; the squared distance of a pair near the cutoff
+    // c is off by at most sum(2|dx| de + de^2) + 3 c^2 2^-23.  The bound used
+    // is four times that, with c the larger cutoff.
+    {
+        double ext = std::max(f.xmax - f.xmin, f.ymax - f.ymin);
+        if (f.dim == 3) ext = std::max(ext, f.zmax - f.zmin);
+        double cmax = std::max(f.re_l, f.re_s) + (f.dim == 3 ? f.delta : 0.0);
+        double u = std::ldexp(1.0, -24);
+        double de = 2 * ext * u + cmax * u;
+        c->screen_abs = 4.0 * (3 * (2 * cmax * de + de * de) + 3 * cmax * cmax * 2 * u);
     }
     bool strict = f.dim == 2;
     c->cut_l = sqrt_cut(strict ? f.re_l : f.re_l + f.delta, strict);

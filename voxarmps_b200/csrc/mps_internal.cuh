@@ -115,6 +115,8 @@ struct mps_ctx {
     // packed gathers: positions (x, y, z, ptype), predicted positions,
     // collision output, velocities (u, v, w, -) and (pnew, phat) pairs
     double4 *P4 = nullptr, *P4s = nullptr, *P4c = nullptr, *U4 = nullptr;
+    float4* P4f = nullptr;   // positions relative to the box minimum, FP32 (list screening)
+    double screen_abs = 0;   // bound on |d2_fp32 - d2_exact| for the screening test
     double2* PH = nullptr;
     // sort / cells
     int *cell_l = nullptr, *cell_s = nullptr;      // per slot, 1-based Cnum

@@ -15,6 +15,7 @@
 //                  ascending id inside a cell), membership decided with the
 //                  reference's exact FP64 arithmetic; a warp per particle for
 //                  the Laplacian radius, GS lanes for the PND radius.
+#include <cmath>
 #include <cstdio>
 
 #include "mps_internal.cuh"
@@ -206,7 +207,8 @@ __global__ void k_translate(int n, const int* __restrict__ inv, const int* __res
 // own order (x offset outermost, ascending id per cell) is restored when
 // lists are exported (mps_download_lists).
 template <int DIM, int G>
-__global__ void k_lists(int n, Grid g, double cut, int cap, const double4* __restrict__ P4,
+__global__ void k_lists(int n, Grid g, double cut, float cut_lo, float cut_hi, int cap,
+                        const double4* __restrict__ P4, const float4* __restrict__ P4f,
                         const int* __restrict__ cell, const int* __restrict__ cst,
                         const int* __restrict__ cnt, const int* __restrict__ perm,
                         int* __restrict__ out, int* __restrict__ len, int* len_max, int which,
@@ -216,6 +218,7 @@ __global__ void k_lists(int n, Grid g, double cut, int cap, const double4* __res
     int i = (int)q.gid;
     if (i >= n) return;  // whole groups leave together (n rows, G lanes each)
     double4 pi = P4[i];
+    float4 fi = P4f[i];
     int C = cell[i] - 1;
     int ic = C % g.ncx + 1, jc = (C / g.ncx) % g.ncy + 1, kc = C / (g.ncx * g.ncy) + 1;
     int m1 = (ic == 1) ? 0 : -1, m2 = (ic == g.ncx) ? 0 : 1;
@@ -254,10 +257,19 @@ __global__ void k_lists(int n, Grid g, double cut, int cap, const double4* __res
                 int j = 0;
                 if (jj < e) {
                     j = perm ? perm[jj] : jj;
-                    double4 pj = P4[j];
-                    double d2 = dist2<DIM>(pj.x - pi.x, pj.y - pi.y,
-                                           DIM == 3 ? pj.z - pi.z : 0.0);
-                    in = (DIM == 3) ? (d2 <= cut) : (j != i && d2 < cut);
+                    // FP32 screen; the exact FP64 rule decides only inside
+                    // the screening margin [cut_lo, cut_hi]
+                    float4 fj = P4f[j];
+                    float ex = fj.x - fi.x, ey = fj.y - fi.y, ez = DIM == 3 ? fj.z - fi.z : 0.f;
+                    float f2 = ex * ex + ey * ey + ez * ez;
+                    if (f2 < cut_lo) {
+                        in = (DIM == 3) || (j != i);
+                    } else if (f2 <= cut_hi) {
+                        double4 pj = P4[j];
+                        double d2 = dist2<DIM>(pj.x - pi.x, pj.y - pi.y,
+                                               DIM == 3 ? pj.z - pi.z : 0.0);
+                        in = (DIM == 3) ? (d2 <= cut) : (j != i && d2 < cut);
+                    }
                 }
                 unsigned m = q.ballot(in);
                 if (in) {
@@ -371,24 +383,30 @@ int vmps_neighbors(mps_ctx* ctx)
     if (ctx->profile) VMPS_CUDA(ctx, cudaEventRecord(ctx->ev[6], st));
     {
         const int n32 = (int)(((long)n * 32 + kBlock - 1) / kBlock);
+        // screening window, rounded outwards to float
+        auto lo = [&](double c) { return std::nextafter((float)(c - ctx->screen_abs), 0.f); };
+        auto hi = [&](double c) { return std::nextafter((float)(c + ctx->screen_abs), INFINITY); };
+        float lo_l = lo(ctx->cut_l), hi_l = hi(ctx->cut_l), lo_s = lo(ctx->cut_s), hi_s = hi(ctx->cut_s);
         if (ctx->cfg.dim == 3) {
             constexpr int GS = SmallG<3>::G;
-            k_lists<3, 32><<<n32, kBlock, 0, st>>>(n, ctx->gl, ctx->cut_l, ctx->cap_l, ctx->P4,
-                                                   ctx->cell_l, ctx->cst_l, ctx->cnt_l, nullptr,
-                                                   ctx->nbr_l, ctx->len_l, ctx->len_max, 0,
-                                                   ctx->d_err);
+            k_lists<3, 32><<<n32, kBlock, 0, st>>>(n, ctx->gl, ctx->cut_l, lo_l, hi_l, ctx->cap_l,
+                                                   ctx->P4, ctx->P4f, ctx->cell_l, ctx->cst_l,
+                                                   ctx->cnt_l, nullptr, ctx->nbr_l, ctx->len_l,
+                                                   ctx->len_max, 0, ctx->d_err);
             k_lists<3, GS><<<(int)(((long)n * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
-                n, ctx->gs, ctx->cut_s, ctx->cap_s, ctx->P4, ctx->cell_s, ctx->cst_s, ctx->cnt_s,
-                ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1, ctx->d_err);
+                n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,
+                ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
+                ctx->d_err);
         } else {
             constexpr int GS = SmallG<2>::G;
-            k_lists<2, 32><<<n32, kBlock, 0, st>>>(n, ctx->gl, ctx->cut_l, ctx->cap_l, ctx->P4,
-                                                   ctx->cell_l, ctx->cst_l, ctx->cnt_l, nullptr,
-                                                   ctx->nbr_l, ctx->len_l, ctx->len_max, 0,
-                                                   ctx->d_err);
+            k_lists<2, 32><<<n32, kBlock, 0, st>>>(n, ctx->gl, ctx->cut_l, lo_l, hi_l, ctx->cap_l,
+                                                   ctx->P4, ctx->P4f, ctx->cell_l, ctx->cst_l,
+                                                   ctx->cnt_l, nullptr, ctx->nbr_l, ctx->len_l,
+                                                   ctx->len_max, 0, ctx->d_err);
             k_lists<2, GS><<<(int)(((long)n * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
-                n, ctx->gs, ctx->cut_s, ctx->cap_s, ctx->P4, ctx->cell_s, ctx->cst_s, ctx->cnt_s,
-                ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1, ctx->d_err);
+                n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,
+                ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
+                ctx->d_err);
         }
     }
     vmps_count_launch(2);

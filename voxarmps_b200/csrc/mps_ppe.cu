@@ -60,7 +60,7 @@ struct Asm {
 // one warp per row; the non-zero columns are compacted in list order into
 // the row's CSR segment (capacity = the row's list length)
 template <int DIM>
-__global__ void k_assemble(int n, int cap, Asm A, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(256, 5) k_assemble(int n, int cap, Asm A, const int* __restrict__ nbr,
                            const int* __restrict__ len, const int* __restrict__ bcon,
                            const double4* __restrict__ P4, const double* __restrict__ nsrc,
                            int warm, double* __restrict__ pnew, const int* __restrict__ moff,
@@ -188,9 +188,11 @@ struct CG {
     int cap, n, precond, nparts;
 };
 
-// (A v)_i with one warp on row i of the CSR matrix: two column/value loads
-// per lane in flight, gathers of v from L2, butterfly sum in a fixed order;
-// every lane returns the row's value.
+// (A v)_i with one warp on row i of the CSR matrix: coalesced column/value
+// streams, two independent accumulators per lane, gathers of v from L2,
+// butterfly sum in a fixed order; every lane returns the row's value.  (This
+// plain form runs at 32 registers; restructured or deeper-unrolled variants
+// measured 15-70% slower on B200.)
 __device__ __forceinline__ double spmv_row_warp(const CG& A, const Grp<32>& q,
                                                 const double* __restrict__ v, int i)
 {
@@ -265,7 +267,7 @@ __global__ void k_cg_start_scalars(int nparts, const double* __restrict__ part, 
     }
 }
 
-// s = A p and partial p.s
+// s = A p and partial p.s; one warp per row
 __global__ void k_cg_spmv(CG A, const double* __restrict__ p, double* __restrict__ s,
                           double* __restrict__ part, const int* __restrict__ flag)
 {

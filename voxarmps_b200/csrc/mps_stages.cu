@@ -699,8 +699,20 @@ inline int group_blocks(long n, int G) { return (int)((n * G + kBlock - 1) / kBl
 
 }  // namespace
 
+__global__ void k_pack_f(int n, const double* __restrict__ x, const double* __restrict__ y,
+                         const double* __restrict__ z, double x0, double y0, double z0,
+                         float4* __restrict__ P4f)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) P4f[i] = make_float4((float)(x[i] - x0), (float)(y[i] - y0), (float)(z[i] - z0), 0.f);
+}
+
 int vmps_pack(mps_ctx* c)
 {
+    const mps_config& f = c->cfg;
+    k_pack_f<<<grid_blocks(c->n), kBlock, 0, c->stream>>>(c->n, c->x, c->y, c->z, f.xmin, f.ymin,
+                                                          f.dim == 3 ? f.zmin : 0.0, c->P4f);
+    vmps_count_launch(1);
     k_pack<<<grid_blocks(c->n), kBlock, 0, c->stream>>>(c->n, c->x, c->y, c->z, c->ptype, c->P4);
     k_pack<<<grid_blocks(c->n), kBlock, 0, c->stream>>>(c->n, c->u, c->v, c->w, nullptr, c->U4);
     vmps_count_launch(2);
