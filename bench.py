@@ -33,9 +33,11 @@ sys.path.insert(0, ROOT)
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 METRIC = "particle-steps/s"
-# ncu capture of k_cg_spmv (profiles/cg_spmv_dam3d.md): DRAM bytes per launch
-# scaled to the full workload by non-zeros; None until a capture exists.
-SPMV_TRAFFIC_BYTES_PER_NNZ = None
+# ncu capture of k_cg_spmv on the 476,608-particle dam (profiles/
+# cg_spmv_dam3d_476k.md): dram read+write per launch / algorithmic bytes of
+# that launch.  The traffic grows with the non-zeros, so the full launch's
+# traffic is this ratio times its algorithmic bytes.
+SPMV_TRAFFIC_OVER_ALGORITHMIC = 812.35 / 741.87
 
 
 def dist_env():
@@ -266,7 +268,7 @@ def run_ours(args):
     spmv_avg_ms = spmv_ms / max(spmv_n, 1)
     algo = spmv_algorithmic_bytes(nnz_a, rows)
     achieved = algo / (spmv_avg_ms * 1e-3) / 1e9 if spmv_n else None
-    traffic = (SPMV_TRAFFIC_BYTES_PER_NNZ * nnz_a) if SPMV_TRAFFIC_BYTES_PER_NNZ else None
+    traffic = SPMV_TRAFFIC_OVER_ALGORITHMIC * algo
     line = None
     if rank == 0:
         cpu = time_reference(steps=3, warmup=1, nthreads=os.cpu_count() or 1) if ws == 1 else None
@@ -285,7 +287,7 @@ def run_ours(args):
             "ppe_ms_per_step": statistics.mean(ppe_ms), "cg_iters_mean": statistics.mean(iters),
             "cg_relres_last": relres, "status_bits": status,
             "stage_ms": {k[3:]: statistics.mean(v) for k, v in stage.items()},
-            "roofline": {"kernel": "k_cg_spmv (PPE SpMV, FP64 slot-major ELL)", "bound": "hbm",
+            "roofline": {"kernel": "k_cg_spmv (PPE SpMV, FP64 CSR, warp per row)", "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
                          "traffic": traffic, "peak_source": peak_kind,
