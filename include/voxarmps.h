@@ -66,7 +66,7 @@ typedef struct mps_config {
     int matopt, srcopt;   /* HL Laplacian, HS+ECS source */
     int fraction_method;  /* 1 linear, 2 kernel-smoothed */
     int ppe_at_predicted; /* 1: A at x*, b from n* (reference GPU path); 0: CPU path */
-    int warm_start;       /* 1: CG starts from the previous pressure */
+    int warm_start;       /* CG initial guess: 0 zero, 1 previous pressure, 2 2p^n - p^(n-1) */
     int solver;           /* 1 Jacobi-PCG, 2 unpreconditioned CG (relative residual) */
     double cg_tol;        /* relative residual ||b-Ax||/||b|| */
     int cg_max;

@@ -973,7 +973,7 @@ struct mo_state {
     mo_params P;
     int n;
     double *x, *y, *z, *u, *v, *w, *p, *pnew, *phat, *un, *vn, *wn, *xs, *ys, *zs, *us, *vs,
-        *ws, *nd, *nds, *C, *meu, *neut, *t1, *t2, *t3, *rho, *source, *diag, *val;
+        *ws, *nd, *nds, *C, *meu, *neut, *t1, *t2, *t3, *rho, *source, *diag, *val, *pold;
     int *ptype, *bcon;
     int *cell_s, *perm_s, *off_s, *nbr_s, cap_s;
     int *cell_l, *perm_l, *off_l, *nbr_l, cap_l;
@@ -1026,7 +1026,7 @@ mo_state* mo_create(const mo_params* P, int n, const double* x, const double* y,
     double** dbl[] = {&S->x,  &S->y,  &S->z,  &S->u,    &S->v,    &S->w,    &S->p,     &S->pnew,
                       &S->phat, &S->un, &S->vn, &S->wn, &S->xs,   &S->ys,   &S->zs,    &S->us,
                       &S->vs, &S->ws, &S->nd, &S->nds, &S->C,   &S->meu,  &S->neut,  &S->t1,
-                      &S->t2, &S->t3, &S->rho, &S->source, &S->diag};
+                      &S->t2, &S->t3, &S->rho, &S->source, &S->diag, &S->pold};
     for (size_t k = 0; k < sizeof(dbl) / sizeof(dbl[0]); k++)
         *dbl[k] = (double*)calloc(nd, sizeof(double));
     S->ptype = (int*)calloc(nd, sizeof(int));
@@ -1062,7 +1062,7 @@ void mo_destroy(mo_state* S)
     double* dbl[] = {S->x,  S->y,  S->z,  S->u,  S->v,   S->w,  S->p,   S->pnew, S->phat, S->un,
                      S->vn, S->wn, S->xs, S->ys, S->zs,  S->us, S->vs,  S->ws,   S->nd,   S->nds,
                      S->C,  S->meu, S->neut, S->t1, S->t2, S->t3, S->rho, S->source, S->diag,
-                     S->val};
+                     S->val, S->pold};
     for (size_t k = 0; k < sizeof(dbl) / sizeof(dbl[0]); k++) free(dbl[k]);
     free(S->ptype); free(S->bcon);
     free(S->cell_s); free(S->perm_s); free(S->off_s); free(S->nbr_s);
@@ -1078,6 +1078,7 @@ int mo_init(mo_state* S)
     S->have_lists = 1;
     mo_pnd(&S->P, S->P.re_s, S->n, S->off_s, S->nbr_s, S->x, S->y, S->z, 1, S->nd);
     for (int i = 0; i < S->n; i++) S->pnew[i] = S->p[i];
+    for (int i = 0; i < S->n; i++) S->pold[i] = S->p[i];
     S->n0_s = mo_max(S->n, S->nd);
     if (single_radius(S)) {
         S->n0_l = S->n0_s;
@@ -1132,7 +1133,14 @@ int mo_step(mo_state* S)
                          ax, ay, az, S->us, S->vs, S->ws, S->source);
         else
             mo_source(P, S->n0_s, n, S->ptype, S->bcon, nsrc, S->source);
-        if (P->warm_start) {
+        if (P->warm_start == 2) {
+            /* linear extrapolation 2 p^n - p^(n-1) on unknown rows */
+            for (int i = 0; i < n; i++) {
+                double pn = S->pnew[i];
+                S->pnew[i] = (S->bcon[i] != 0) ? 0.0 : 2.0 * pn - S->pold[i];
+                S->pold[i] = pn;
+            }
+        } else if (P->warm_start) {
             for (int i = 0; i < n; i++) if (S->bcon[i] != 0) S->pnew[i] = 0.0;
         } else {
             memset(S->pnew, 0, sizeof(double) * (size_t)n);

@@ -56,7 +56,7 @@ typedef struct mo_params {
     /* PPE semantics switches (reference CPU path vs GPU path, see the header
        of mo_step): ppe_at_predicted=1 assembles A at x* and b from n*. */
     int ppe_at_predicted;
-    int warm_start;       /* 1: CG starts from the previous pressure */
+    int warm_start;       /* 0: zero, 1: previous pressure, 2: 2 p^n - p^(n-1) */
     int solver;           /* 0: reference ICCG with its absolute per-row stop rule,
                              1: Jacobi-preconditioned CG to a relative residual,
                              2: unpreconditioned CG to a relative residual */

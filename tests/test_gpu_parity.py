@@ -158,3 +158,15 @@ def test_matopt_srcopt():
         o.step()
         assert rel_err(g.get("source"), o.get("source")) <= 1e-9, kw
         assert rel_err(g.get("p"), o.get("p")) <= 1e-6, kw
+
+
+def test_extrapolated_initial_guess_matches_oracle():
+    """warm_start = 2 (x0 = 2 p^n - p^(n-1)) on both sides, 6 steps."""
+    cfg, case = config.baseline(0)
+    cfg = gpu_cfg(cfg, cg_tol=1e-12, warm_start=2)
+    g, o = pair(cfg, case)
+    for _ in range(6):
+        assert g.step() == 0
+        o.step()
+    for f in ("x", "y", "u", "v", "p"):
+        assert rel_err(g.get(f), o.get(f)) <= 1e-6, f

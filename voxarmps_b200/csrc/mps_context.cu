@@ -119,6 +119,7 @@ int validate(const mps_config& f, std::string& why)
         return MPS_ERR_ARG;
     }
     if (f.solver != 1 && f.solver != 2) { why = "solver must be 1 (Jacobi-PCG) or 2 (CG)"; return MPS_ERR_ARG; }
+    if (f.warm_start < 0 || f.warm_start > 2) { why = "warm_start must be 0, 1 or 2"; return MPS_ERR_ARG; }
     if (f.precision != 0) { why = "precision 1 (mixed) is not available in this build"; return MPS_ERR_ARG; }
     return MPS_OK;
 }
@@ -198,7 +199,7 @@ int allocate(mps_ctx* c)
 {
     const size_t P = (size_t)c->pitch;
     double** dfields[] = {&c->x, &c->y, &c->z, &c->u, &c->v, &c->w, &c->p, &c->pnew,
-                          &c->phat, &c->un, &c->vn, &c->wn, &c->rho, &c->nd, &c->xs, &c->ys,
+                          &c->phat, &c->un, &c->vn, &c->wn, &c->rho, &c->nd, &c->pold, &c->xs, &c->ys,
                           &c->zs, &c->us, &c->vs, &c->ws, &c->nds, &c->C, &c->meu, &c->neut,
                           &c->t1, &c->t2, &c->t3, &c->source, &c->diag, &c->cg_r, &c->cg_z,
                           &c->cg_p, &c->cg_s, &c->xc, &c->yc, &c->zc, &c->uc, &c->vc, &c->wc,
@@ -242,9 +243,9 @@ int allocate(mps_ctx* c)
     TRY(halloc(c, &c->red_host, 16));
     TRY(halloc(c, &c->h_err, 1));
     // alternates of the persistent fields for the reorder (same order as
-    // persistent_set in mps_neighbors.cu: 14 doubles then 4 ints)
+    // persistent_set in mps_neighbors.cu: 15 doubles then 4 ints)
     c->alts.clear();
-    for (int k = 0; k < 14; k++) {
+    for (int k = 0; k < 15; k++) {
         double* q;
         TRY(dalloc(c, &q, P));
         c->alts.push_back(q);
@@ -452,6 +453,8 @@ int mps_init(mps_ctx* c)
         TRY(device_max(c, &c->n0_l));
     }
     VMPS_CUDA(c, cudaMemcpyAsync(c->pnew, c->p, sizeof(double) * c->n, cudaMemcpyDeviceToDevice,
+                                 c->stream));
+    VMPS_CUDA(c, cudaMemcpyAsync(c->pold, c->p, sizeof(double) * c->n, cudaMemcpyDeviceToDevice,
                                  c->stream));
     c->initialized = true;
     int e = collect_errors(c);

@@ -101,7 +101,7 @@ struct mps_ctx {
     // persistent particle state, cell order (double-buffered for the reorder)
     double *x = nullptr, *y = nullptr, *z = nullptr, *u = nullptr, *v = nullptr, *w = nullptr;
     double *p = nullptr, *pnew = nullptr, *phat = nullptr, *un = nullptr, *vn = nullptr,
-           *wn = nullptr, *rho = nullptr, *nd = nullptr;
+           *wn = nullptr, *rho = nullptr, *nd = nullptr, *pold = nullptr;
     int *ptype = nullptr, *oid = nullptr;
     // per-step scratch fields
     double *xs = nullptr, *ys = nullptr, *zs = nullptr, *us = nullptr, *vs = nullptr,

@@ -315,7 +315,7 @@ static void persistent_set(mps_ctx* ctx, GatherSet& g, std::vector<void**>& slot
     g.count = 0;
     slots.clear();
     double** d[] = {&ctx->x, &ctx->y, &ctx->z, &ctx->u, &ctx->v, &ctx->w, &ctx->p, &ctx->pnew,
-                    &ctx->phat, &ctx->un, &ctx->vn, &ctx->wn, &ctx->rho, &ctx->nd};
+                    &ctx->phat, &ctx->un, &ctx->vn, &ctx->wn, &ctx->rho, &ctx->nd, &ctx->pold};
     int** ii[] = {&ctx->ptype, &ctx->oid, &ctx->cell_l, &ctx->cell_s};
     for (auto f : d) {
         g.from[g.count] = *f;

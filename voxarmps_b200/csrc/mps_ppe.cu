@@ -63,7 +63,8 @@ template <int DIM>
 __global__ void __launch_bounds__(256, 5) k_assemble(int n, int cap, Asm A, const int* __restrict__ nbr,
                            const int* __restrict__ len, const int* __restrict__ bcon,
                            const double4* __restrict__ P4, const double* __restrict__ nsrc,
-                           int warm, double* __restrict__ pnew, const int* __restrict__ moff,
+                           int warm, double* __restrict__ pnew, double* __restrict__ pold,
+                           const int* __restrict__ moff,
                            int* __restrict__ mcol, double* __restrict__ mval,
                            int* __restrict__ mlen, double* __restrict__ diag,
                            double* __restrict__ source)
@@ -77,6 +78,7 @@ __global__ void __launch_bounds__(256, 5) k_assemble(int n, int cap, Asm A, cons
             mlen[i] = 0;
             diag[i] = 0.0;
             source[i] = 0.0;
+            if (warm == 2) pold[i] = pnew[i];
             pnew[i] = 0.0;
         }
         return;
@@ -119,7 +121,15 @@ __global__ void __launch_bounds__(256, 5) k_assemble(int n, int cap, Asm A, cons
         diag[i] = dg + A.reg;
         mlen[i] = cnt;
         if (!A.srcopt) source[i] = 1.0 / A.dt / A.dt * (nsrc[i] - A.n0_s) / A.n0_s;
-        if (!warm) pnew[i] = 0.0;
+        // initial guess: 0, the previous pressure, or the linear extrapolation
+        // 2 p^n - p^(n-1) (pold keeps p^n for the next step)
+        if (!warm) {
+            pnew[i] = 0.0;
+        } else if (warm == 2) {
+            double pn = pnew[i];
+            pnew[i] = 2.0 * pn - pold[i];
+            pold[i] = pn;
+        }
     }
 }
 
@@ -401,11 +411,11 @@ int vmps_ppe(mps_ctx* c)
     const int wblocks = (int)(((long)n * 32 + kBlock - 1) / kBlock);
     if (f.dim == 3)
         k_assemble<3><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
-                                                  nsrc, f.warm_start, c->pnew, c->moff, c->mcol,
+                                                  nsrc, f.warm_start, c->pnew, c->pold, c->moff, c->mcol,
                                                   c->mval, c->mlen, c->diag, c->source);
     else
         k_assemble<2><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
-                                                  nsrc, f.warm_start, c->pnew, c->moff, c->mcol,
+                                                  nsrc, f.warm_start, c->pnew, c->pold, c->moff, c->mcol,
                                                   c->mval, c->mlen, c->diag, c->source);
     vmps_count_launch(1);
     if (f.srcopt) {
