@@ -116,15 +116,35 @@ def spmv_algorithmic_bytes(nnz_a: float, rows: float) -> float:
     return nnz_a * 12.0 + rows * 32.0
 
 
-def build_case(scale: int = 0):
-    """The benchmark scene; scale > 0 selects the smaller 3D dam used for
-    profiling captures (config.scaled_dam3d)."""
+WORKLOADS = {
+    0: "2D dam break, 25x50 fluid (1,250) + 678 wall/dummy particles, l0=0.01, "
+       "re=2.1/4.0*l0, dt=1e-4, FP64 Jacobi-PCG to 1e-8",
+    1: "3D dam break, 80x160x80 fluid (1,024,000) + 571,308 wall/dummy particles, l0=0.005, "
+       "re=2.1/4.0*l0, dt=5e-5, FP64 Jacobi-PCG to 1e-8 relative residual",
+    3: "2D two-phase dam, water 600x100 + Bingham block 150x150 (82,500 fluid), l0=0.002, "
+       "SPS-LES Cs=0.12, HB second fluid, dt=1e-4, FP64 Jacobi-PCG to 1e-8",
+    4: "64 batched 2D dam breaks (splitmix64 seed 0, columns U[0.1,0.4]x U[0.2,0.6] m, "
+       "l0=0.005), one context, every scene's PPE to 1e-8",
+}
+
+
+def build_case(scale: int = 0, which: int = 1):
+    """(cfg, case, scenes) of the benchmark scene; scale > 0 selects the
+    smaller 3D dam used for profiling captures (config.scaled_dam3d)."""
     from voxarmps_b200 import config
-    cfg, case = config.scaled_dam3d(scale) if scale else config.baseline(1)
+    scenes = None
+    if scale:
+        cfg, case = config.scaled_dam3d(scale)
+    elif which == 4:
+        base, sc = config.baseline(4)
+        cfg, case, sid, boxes, pmax = config.batched(base, sc)
+        scenes = (sid, boxes, pmax)
+    else:
+        cfg, case = config.baseline(which)
     cfg = config.solver_semantics(cfg)
     cfg["cg_tol"] = 1e-8
     cfg["cg_max"] = 1000
-    return cfg, case
+    return cfg, case, scenes
 
 
 def cpu_reference_sample():
@@ -197,10 +217,12 @@ def run_ours(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    cfg, case = build_case(args.scale)
+    cfg, case, scenes = build_case(args.scale, args.config)
     n = len(case["x"])
     fp = int((case["ptype"] > 0).sum())
     s = vm.Solver(cfg, case, device=dev)
+    if scenes is not None:
+        s.set_scenes(*scenes)
     s.init()
     s.set_profile(True)
     stream = torch.cuda.ExternalStream(s.stream())
@@ -271,15 +293,15 @@ def run_ours(args):
     traffic = SPMV_TRAFFIC_OVER_ALGORITHMIC * algo
     line = None
     if rank == 0:
-        cpu = time_reference(steps=3, warmup=1, nthreads=os.cpu_count() or 1) if ws == 1 else None
+        cpu = (time_reference(steps=3, warmup=1, nthreads=os.cpu_count() or 1)
+               if ws == 1 and args.config == 1 and not args.scale else None)
         value = n * args.steps * ws / (el_ms * 1e-3)
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": el_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "3D dam break, 80x160x80 fluid (1,024,000) + 571,308 wall/"
-                                   "dummy particles, l0=0.005, re=2.1/4.0*l0, dt=5e-5, "
-                                   "FP64 Jacobi-PCG to 1e-8 relative residual",
+            "config": {"workload": (WORKLOADS[args.config] if not args.scale else
+                                    f"3D dam break scaled x{args.scale} (profiling case)"),
                        "particles": n, "fluid_particles": fp,
                        "parallelism": f"{ws} independent scenes" if ws > 1 else "1 scene",
                        "l2": "working set (lists, matrix) > 126 MB L2; no flush needed"},
@@ -313,6 +335,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 3, 4],
+                    help="benchmark configuration (1: the headline 3D dam break)")
     ap.add_argument("--scale", type=int, default=0,
                     help="profiling only: smaller 3D dam (10s x 20s x 10s fluid)")
     args = ap.parse_args()

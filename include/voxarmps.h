@@ -94,6 +94,19 @@ int mps_upload(mps_ctx* ctx, int n, const double* x, const double* y, const doub
 /* Read a .grd file (main.cu:496-684 format) and upload it. */
 int mps_load_grd(mps_ctx* ctx, const char* path);
 
+/* Batched independent scenes (no reference counterpart: the reference runs
+ * one scene per process).  Call after mps_upload and before mps_init.
+ * scene[i] in [0, nscenes): the scene of particle i (caller order); boxes:
+ * 6 doubles per scene (xmin xmax ymin ymax zmin zmax, the grown box of
+ * main.cu:692-715); pmax: one per scene (main.cu:548).  Scenes share one
+ * cell grid and must be separated by more than re_l so that no list
+ * crosses scenes; they must share spacing, radii and kernel (one n0).
+ * Wall clamps, the box check and the pressure cap use each particle's
+ * scene; the PPE is solved until every scene's own relative residual is
+ * <= cg_tol. */
+int mps_set_scenes(mps_ctx* ctx, int nscenes, const int* scene, const double* boxes,
+                   const double* pmax);
+
 /* Pre-iteration work (main.cu:964-1012): density, lists, n0 = max PND. */
 int mps_init(mps_ctx* ctx);
 

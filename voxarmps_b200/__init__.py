@@ -44,7 +44,7 @@ EXPORTS = [
     "mps_integrate", "mps_collision", "mps_commit", "mps_step", "mps_run", "mps_download",
     "mps_download_lists", "mps_get_scalar", "mps_get_error", "mps_last_message",
     "mps_write_vtu", "mps_stream", "mps_set_state", "mps_get_state", "mps_set_profile",
-    "mps_cell_order_noalloc",
+    "mps_cell_order_noalloc", "mps_set_scenes",
 ]
 
 _LIB = None
@@ -89,6 +89,8 @@ def load_library(path: str = LIB_PATH):
     lib.mps_set_state.argtypes = [P, P, P, P, P, P, P, P]
     lib.mps_get_state.argtypes = [P, P, P, P, P, P, P, P]
     lib.mps_set_profile.argtypes = [P, C.c_int]
+    lib.mps_set_scenes.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                   C.POINTER(C.c_double)]
     lib.mps_cell_order_noalloc.argtypes = [C.POINTER(MpsConfig), C.c_double, C.c_int, P, P, P,
                                            P, P, P, P]
     _LIB = lib
@@ -131,6 +133,17 @@ class Solver:
                                       pt.ctypes.data_as(C.POINTER(C.c_int)), _dp(u), _dp(v),
                                       _dp(w), _dp(p)), "upload")
         self.n = n
+        return self
+
+    def set_scenes(self, scene, boxes, pmax):
+        """Batched independent scenes (after upload, before init)."""
+        sc = np.ascontiguousarray(scene, np.int32)
+        bx = np.ascontiguousarray(boxes, np.float64).reshape(-1)
+        pm = np.ascontiguousarray(pmax, np.float64)
+        self._scenes = (sc, bx, pm)
+        self._chk(self.lib.mps_set_scenes(self.h, len(pm), sc.ctypes.data_as(C.POINTER(C.c_int)),
+                                          bx.ctypes.data_as(C.POINTER(C.c_double)),
+                                          pm.ctypes.data_as(C.POINTER(C.c_double))), "scenes")
         return self
 
     def load_grd(self, path: str):

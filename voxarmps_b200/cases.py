@@ -150,6 +150,41 @@ def batched_dam_scenes(count: int = 64, seed: int = 0, l0: float = 0.005):
     return scenes
 
 
+def stack_scenes(scenes, gap: float):
+    """Independent scenes in one domain, stacked along y with ``gap`` metres
+    of empty space between neighbouring scenes (gap > the largest support
+    radius keeps every neighbour list inside its scene, and each scene then
+    occupies whole cell rows, i.e. a contiguous range of the cell order).
+
+    Returns (case, scene_of_particle, boxes, pmax): boxes holds each scene's
+    grown box (main.cu:692-715) after the shift, pmax = TP*4.5 per scene
+    (main.cu:548)."""
+    dim = scenes[0]["dim"]
+    dl = scenes[0]["l0"]
+    parts = {k: [] for k in ("x", "y", "z", "u", "v", "w", "p", "ptype")}
+    scene_id, boxes, pmax = [], [], []
+    y0 = 0.0
+    for k, sc in enumerate(scenes):
+        ys = np.asarray(sc["y"])
+        shift = y0 - ys.min()
+        for key in parts:
+            a = np.asarray(sc[key])
+            parts[key].append(a + shift if key == "y" else a)
+        scene_id.append(np.full(len(ys), k, np.int32))
+        x = np.asarray(sc["x"])
+        z = np.asarray(sc["z"])
+        box = [x.min() - dl, x.max() + dl, ys.min() + shift - dl, ys.max() + shift + dl]
+        box += [z.min() - dl, z.max() + dl] if dim == 3 else [99999999.0, -99999999.0]
+        boxes.append(box)
+        pmax.append(len(ys) * 4.50)
+        y0 = ys.max() + shift + gap
+    case = {key: np.concatenate(v) for key, v in parts.items()}
+    case["ptype"] = case["ptype"].astype(np.int32)
+    case["dim"], case["l0"] = dim, dl
+    return (case, np.concatenate(scene_id), np.asarray(boxes, np.float64),
+            np.asarray(pmax, np.float64))
+
+
 def lattice_neighbours(dim: int, ratio: float, inclusive: bool = False) -> int:
     """Number of lattice nodes within ratio*l0 of a node (self excluded)."""
     r = int(math.ceil(ratio)) + 1

@@ -122,6 +122,22 @@ def baseline(idx: int):
     return with_box(cfg, case), case
 
 
+def batched(cfg: dict, scenes, gap_radii: float = 4.0):
+    """(cfg, stacked case, scene ids, boxes, pmax) for scenes advanced in one
+    context; the gap between scenes is gap_radii Laplacian radii."""
+    case, sid, boxes, pmax = cases.stack_scenes(scenes, gap_radii * cfg["re_l"])
+    c = dict(cfg)
+    c["xmin"], c["xmax"] = float(boxes[:, 0].min()), float(boxes[:, 1].max())
+    c["ymin"], c["ymax"] = float(boxes[:, 2].min()), float(boxes[:, 3].max())
+    if c["dim"] == 3:
+        c["zmin"], c["zmax"] = float(boxes[:, 4].min()), float(boxes[:, 5].max())
+    else:
+        c["zmin"], c["zmax"] = 99999999.0, -99999999.0
+    c["pmax"] = float(pmax.max())
+    return c, case, sid, boxes, pmax
+
+
+
 def scaled_dam3d(scale: int, l0: float = 0.005):
     """3D dam with the config-1 spacing and radii and a 10s x 20s x 10s column in
     a proportionally smaller tank (the bounded CPU sample)."""

@@ -205,7 +205,7 @@ int allocate(mps_ctx* c)
                           &c->cg_p, &c->cg_s, &c->xc, &c->yc, &c->zc, &c->uc, &c->vc, &c->wc,
                           &c->pres_x, &c->pres_y, &c->pres_z};
     for (auto f : dfields) TRY(dalloc(c, f, P));
-    int** ifields[] = {&c->ptype, &c->oid, &c->bcon, &c->cell_l, &c->cell_s, &c->bpos_l,
+    int** ifields[] = {&c->ptype, &c->oid, &c->scene, &c->bcon, &c->cell_l, &c->cell_s, &c->bpos_l,
                        &c->bpos_s, &c->bslot_l, &c->boid_l, &c->bslot_s, &c->boid_s, &c->src,
                        &c->inv, &c->perm_s, &c->perm_s_tmp, &c->len_l, &c->len_s, &c->mlen,
                        &c->moff};
@@ -243,14 +243,14 @@ int allocate(mps_ctx* c)
     TRY(halloc(c, &c->red_host, 16));
     TRY(halloc(c, &c->h_err, 1));
     // alternates of the persistent fields for the reorder (same order as
-    // persistent_set in mps_neighbors.cu: 15 doubles then 4 ints)
+    // persistent_set in mps_neighbors.cu: 15 doubles then 5 ints)
     c->alts.clear();
     for (int k = 0; k < 15; k++) {
         double* q;
         TRY(dalloc(c, &q, P));
         c->alts.push_back(q);
     }
-    for (int k = 0; k < 4; k++) {
+    for (int k = 0; k < 5; k++) {
         int* q;
         TRY(dalloc(c, &q, P));
         c->alts.push_back(q);
@@ -325,6 +325,7 @@ int mps_upload(mps_ctx* c, int n, const double* x, const double* y, const double
     free_all(c);
     mps_config& f = c->cfg;
     c->n = n;
+    c->nscenes = 1;
     c->pitch = (n + 31) / 32 * 32;
     c->gp = c->wp = c->fp = 0;
     for (int i = 0; i < n; i++) {
@@ -399,6 +400,34 @@ int mps_upload(mps_ctx* c, int n, const double* x, const double* y, const double
     c->initialized = false;
     c->steps = 0;
     c->host_err = 0;
+    return MPS_OK;
+}
+
+int mps_set_scenes(mps_ctx* c, int nscenes, const int* scene, const double* boxes,
+                   const double* pmax)
+{
+    // particles must still be in caller order: after mps_upload, before mps_init
+    if (!c || c->n == 0 || c->initialized || nscenes < 1 || !scene || !boxes || !pmax)
+        return MPS_ERR_ARG;
+    for (int i = 0; i < c->n; i++)
+        if (scene[i] < 0 || scene[i] >= nscenes) return MPS_ERR_ARG;
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    c->nscenes = nscenes;
+    TRY(dalloc(c, &c->sbox, (size_t)6 * nscenes));
+    TRY(dalloc(c, &c->spmax, (size_t)nscenes));
+    TRY(dalloc(c, &c->sfirst, (size_t)nscenes));
+    TRY(dalloc(c, &c->slast, (size_t)nscenes));
+    TRY(dalloc(c, &c->sbb, (size_t)nscenes));
+    TRY(dalloc(c, &c->srr, (size_t)nscenes));
+    TRY(dalloc(c, &c->sok, (size_t)nscenes));
+    cudaStream_t st = c->stream;
+    VMPS_CUDA(c, cudaMemcpyAsync(c->sbox, boxes, sizeof(double) * 6 * nscenes,
+                                 cudaMemcpyHostToDevice, st));
+    VMPS_CUDA(c, cudaMemcpyAsync(c->spmax, pmax, sizeof(double) * nscenes, cudaMemcpyHostToDevice,
+                                 st));
+    // scene of slot i: the upload left particles in caller order (oid = i)
+    VMPS_CUDA(c, cudaMemcpyAsync(c->scene, scene, sizeof(int) * c->n, cudaMemcpyHostToDevice, st));
+    VMPS_CUDA(c, cudaStreamSynchronize(st));
     return MPS_OK;
 }
 

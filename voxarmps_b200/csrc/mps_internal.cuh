@@ -102,7 +102,15 @@ struct mps_ctx {
     double *x = nullptr, *y = nullptr, *z = nullptr, *u = nullptr, *v = nullptr, *w = nullptr;
     double *p = nullptr, *pnew = nullptr, *phat = nullptr, *un = nullptr, *vn = nullptr,
            *wn = nullptr, *rho = nullptr, *nd = nullptr, *pold = nullptr;
-    int *ptype = nullptr, *oid = nullptr;
+    int *ptype = nullptr, *oid = nullptr, *scene = nullptr;
+    // batched scenes (nscenes == 1: one scene, the global box)
+    int nscenes = 1;
+    double* sbox = nullptr;     // 6 per scene
+    double* spmax = nullptr;    // per scene
+    int *sfirst = nullptr, *slast = nullptr;  // slot range of each scene
+    double* sbb = nullptr;      // per-scene b.b
+    double* srr = nullptr;      // per-scene r.r
+    int* sok = nullptr;         // per-scene converged flag
     // per-step scratch fields
     double *xs = nullptr, *ys = nullptr, *zs = nullptr, *us = nullptr, *vs = nullptr,
            *ws = nullptr, *nds = nullptr, *C = nullptr, *meu = nullptr, *neut = nullptr,

@@ -189,6 +189,23 @@ __global__ void k_gather(int n, const int* __restrict__ src, GatherSet g)
     }
 }
 
+__global__ void k_scene_ranges_init(int ns, int n, int* __restrict__ first, int* __restrict__ last)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < ns) { first[k] = n; last[k] = 0; }
+}
+
+// slot range [first, last) of each scene after the reorder
+__global__ void k_scene_ranges(int n, const int* __restrict__ scene, int* __restrict__ first,
+                               int* __restrict__ last)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int s = scene[k];
+    atomicMin(&first[s], k);
+    atomicMax(&last[s], k + 1);
+}
+
 __global__ void k_translate(int n, const int* __restrict__ inv, const int* __restrict__ in,
                             int* __restrict__ out)
 {
@@ -316,7 +333,7 @@ static void persistent_set(mps_ctx* ctx, GatherSet& g, std::vector<void**>& slot
     slots.clear();
     double** d[] = {&ctx->x, &ctx->y, &ctx->z, &ctx->u, &ctx->v, &ctx->w, &ctx->p, &ctx->pnew,
                     &ctx->phat, &ctx->un, &ctx->vn, &ctx->wn, &ctx->rho, &ctx->nd, &ctx->pold};
-    int** ii[] = {&ctx->ptype, &ctx->oid, &ctx->cell_l, &ctx->cell_s};
+    int** ii[] = {&ctx->ptype, &ctx->oid, &ctx->cell_l, &ctx->cell_s, &ctx->scene};
     for (auto f : d) {
         g.from[g.count] = *f;
         g.elem[g.count] = 8;
@@ -376,6 +393,12 @@ int vmps_neighbors(mps_ctx* ctx)
     }
     k_translate<<<nb, kBlock, 0, st>>>(n, ctx->inv, ctx->perm_s_tmp, ctx->perm_s);
     vmps_count_launch(1);
+    if (ctx->nscenes > 1) {
+        k_scene_ranges_init<<<grid_blocks(ctx->nscenes), kBlock, 0, st>>>(ctx->nscenes, n,
+                                                                          ctx->sfirst, ctx->slast);
+        k_scene_ranges<<<nb, kBlock, 0, st>>>(n, ctx->scene, ctx->sfirst, ctx->slast);
+        vmps_count_launch(2);
+    }
     {
         int r = vmps_pack(ctx);
         if (r != MPS_OK) return r;

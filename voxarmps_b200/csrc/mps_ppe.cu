@@ -335,7 +335,8 @@ __global__ void k_cg_update(CG A, double* __restrict__ x, double* __restrict__ r
 // (nothing read by this kernel is written by it).
 __global__ void k_cg_direction(CG A, const double* __restrict__ zv, double* __restrict__ p,
                                const double* __restrict__ part, double* scal,
-                               const int* __restrict__ flag, double tol2, int maxit)
+                               const int* __restrict__ flag, double tol2, int maxit,
+                               int nscenes, const int* __restrict__ sok)
 {
     __shared__ double sh[33];
     if (flag[0]) return;
@@ -343,7 +344,12 @@ __global__ void k_cg_direction(CG A, const double* __restrict__ zv, double* __re
     double rr = reduce_parts(part + A.nparts, A.nparts, sh);
     double beta = rz / scal[S_RZ];
     int it = flag[1] + 1;
-    bool done = (rr <= tol2 * scal[S_BB]) || it >= maxit || !(rr == rr);
+    bool conv = rr <= tol2 * scal[S_BB];
+    if (nscenes > 1) {  // every scene to its own relative residual
+        conv = true;
+        for (int k = 0; k < nscenes; k++) conv = conv && (sok[k] != 0);
+    }
+    bool done = conv || it >= maxit || !(rr == rr);
     if (!done) {
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x)
             if (A.bcon[i] == 0) p[i] = zv[i] + beta * p[i];
@@ -352,6 +358,32 @@ __global__ void k_cg_direction(CG A, const double* __restrict__ zv, double* __re
         scal[S_NEWRZ] = rz;
         scal[S_NEWRR] = rr;
         scal[S_DONE] = done ? 1.0 : 0.0;
+    }
+}
+
+// Batched scenes: per-scene sums over each scene's slot range (one block per
+// scene, fixed order).  mode 0: b.b -> sbb; mode 1: r.r -> srr and the
+// scene's converged flag sok = (r.r <= tol2 * b.b).
+__global__ void k_scene_sums(int mode, const int* __restrict__ first, const int* __restrict__ last,
+                             const int* __restrict__ scene, const int* __restrict__ bcon,
+                             const double* __restrict__ v, double tol2, double* __restrict__ sbb,
+                             double* __restrict__ srr, int* __restrict__ sok,
+                             const int* __restrict__ flag)
+{
+    __shared__ double sh[33];
+    if (flag && flag[0]) return;
+    int k = blockIdx.x;
+    double acc = 0.0;
+    for (int i = first[k] + threadIdx.x; i < last[k]; i += blockDim.x)
+        if (scene[i] == k && bcon[i] == 0) acc += v[i] * v[i];
+    acc = block_sum(acc, sh);
+    if (threadIdx.x == 0) {
+        if (mode == 0) {
+            sbb[k] = acc;
+        } else {
+            srr[k] = acc;
+            sok[k] = (sbb[k] == 0.0 || acc <= tol2 * sbb[k]) ? 1 : 0;
+        }
     }
 }
 
@@ -372,11 +404,17 @@ __global__ void k_cg_commit(double* scal, int* flag)
 
 // clamp (functions.cu:2534-2547); a zero right-hand side gives p = 0
 __global__ void k_clamp(int n, double pmin, double pmax, const double* __restrict__ scal,
-                        double* __restrict__ pnew)
+                        double* __restrict__ pnew, const int* __restrict__ scene,
+                        const double* __restrict__ spmax, const double* __restrict__ sbb)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double v = scal[S_ZERO] != 0.0 ? 0.0 : pnew[i];
+    if (scene) {  // batched: the scene's own cap, zero where its right-hand side is zero
+        int k = scene[i];
+        pmax = spmax[k];
+        if (sbb[k] == 0.0) v = 0.0;
+    }
     if (v < pmin) v = pmin;
     if (v > pmax || v * 0.0 != 0.0) v = pmax;
     pnew[i] = v;
@@ -448,6 +486,13 @@ int vmps_ppe(mps_ctx* c)
                                              c->cg_part);
     k_cg_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal, c->cg_flag);
     vmps_count_launch(2);
+    const bool batched = c->nscenes > 1;
+    if (batched) {
+        k_scene_sums<<<c->nscenes, kRedThreads, 0, st>>>(0, c->sfirst, c->slast, c->scene, c->bcon,
+                                                         c->source, tol2, c->sbb, nullptr, nullptr,
+                                                         nullptr);
+        vmps_count_launch(1);
+    }
     const int check = 4;
     int it = 0;
     int nspmv = 0;
@@ -467,8 +512,15 @@ int vmps_ppe(mps_ctx* c)
         k_cg_update<<<nblk, kRedThreads, 0, st>>>(G, c->pnew, c->cg_r, c->cg_z, c->cg_p, c->cg_s,
                                                   c->cg_part + 4 * nblk, c->cg_part, c->cg_scal,
                                                   c->cg_flag);
+        if (batched) {
+            k_scene_sums<<<c->nscenes, kRedThreads, 0, st>>>(1, c->sfirst, c->slast, c->scene,
+                                                             c->bcon, c->cg_r, tol2, c->sbb,
+                                                             c->srr, c->sok, c->cg_flag);
+            vmps_count_launch(1);
+        }
         k_cg_direction<<<nblk, kRedThreads, 0, st>>>(G, c->cg_z, c->cg_p, c->cg_part, c->cg_scal,
-                                                     c->cg_flag, tol2, f.cg_max);
+                                                     c->cg_flag, tol2, f.cg_max, c->nscenes,
+                                                     c->sok);
         k_cg_commit<<<1, 1, 0, st>>>(c->cg_scal, c->cg_flag);
         vmps_count_launch(4);
         if ((it + 1) % check == 0 || it + 1 == f.cg_max) {
@@ -482,7 +534,8 @@ int vmps_ppe(mps_ctx* c)
                                  cudaMemcpyDeviceToHost, st));
     VMPS_CUDA(c, cudaMemcpyAsync(c->red_host, c->cg_scal, S_COUNT * sizeof(double),
                                  cudaMemcpyDeviceToHost, st));
-    k_clamp<<<grid_blocks(n), kBlock, 0, st>>>(n, f.pmin, f.pmax, c->cg_scal, c->pnew);
+    k_clamp<<<grid_blocks(n), kBlock, 0, st>>>(n, f.pmin, f.pmax, c->cg_scal, c->pnew,
+                                               batched ? c->scene : nullptr, c->spmax, c->sbb);
     vmps_count_launch(1);
     VMPS_CUDA(c, cudaStreamSynchronize(st));
     c->cg_iters = c->cg_flag_host[1];
@@ -497,6 +550,17 @@ int vmps_ppe(mps_ctx* c)
     }
     double bb = c->red_host[S_BB], rr = c->red_host[S_RR];
     c->cg_relres = bb > 0 ? sqrt(rr / bb) : 0.0;
+    if (batched) {  // the worst scene's relative residual
+        std::vector<double> hb(c->nscenes), hr(c->nscenes);
+        VMPS_CUDA(c, cudaMemcpy(hb.data(), c->sbb, sizeof(double) * c->nscenes,
+                                cudaMemcpyDeviceToHost));
+        VMPS_CUDA(c, cudaMemcpy(hr.data(), c->srr, sizeof(double) * c->nscenes,
+                                cudaMemcpyDeviceToHost));
+        double worst = 0.0;
+        for (int k = 0; k < c->nscenes; k++)
+            if (hb[k] > 0) worst = std::max(worst, sqrt(hr[k] / hb[k]));
+        c->cg_relres = worst;
+    }
     if (!(c->cg_relres <= f.cg_tol)) c->host_err |= MPS_ERR_NOT_CONVERGED;
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;

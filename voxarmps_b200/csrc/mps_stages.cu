@@ -516,7 +516,20 @@ __global__ void k_pressgrad(int n, Lists L, GradArgs A, const int* __restrict__ 
 
 struct Box {
     double xmin, xmax, ymin, ymax, zmin, zmax, dl, dt, cc;
+    const int* scene;     // per-particle scene, or nullptr for one scene
+    const double* sbox;   // 6 per scene
 };
+
+// the box of particle I: its scene's when scenes are batched
+__device__ __forceinline__ void box_of(const Box& B, int I, double* b)
+{
+    if (B.scene) {
+        const double* q = B.sbox + 6 * B.scene[I];
+        for (int k = 0; k < 6; k++) b[k] = q[k];
+    } else {
+        b[0] = B.xmin; b[1] = B.xmax; b[2] = B.ymin; b[3] = B.ymax; b[4] = B.zmin; b[5] = B.zmax;
+    }
+}
 
 // EULERINTEGRATION + BOUNDARIE (functions.cu:1963-2021)
 template <int DIM>
@@ -528,18 +541,20 @@ __global__ void k_integrate(int n, Box B, const int* __restrict__ ptype, double*
     int I = blockIdx.x * blockDim.x + threadIdx.x;
     if (I >= n || ptype[I] <= 0) return;
     double DT = B.dt, DL = B.dl, CC = B.cc;
+    double bx[6];
+    box_of(B, I, bx);
     double xi = x[I] + un[I] * DT, yi = y[I] + vn[I] * DT;
     double ui = un[I], vi = vn[I];
-    if (yi < B.ymin + DL * 3.0) { vi = fabs(vi) * CC; yi = B.ymin + DL * 3.0; }
-    if (yi > B.ymax - DL * 3.0) { vi = -fabs(vi) * CC; yi = B.ymax - DL * 3.0; }
-    if (xi < B.xmin + DL * 3.0) { ui = fabs(ui) * CC; xi = B.xmin + DL * 3.0; }
-    if (xi > B.xmax - DL * 3.0) { ui = -fabs(ui) * CC; xi = B.xmax - DL * 3.0; }
+    if (yi < bx[2] + DL * 3.0) { vi = fabs(vi) * CC; yi = bx[2] + DL * 3.0; }
+    if (yi > bx[3] - DL * 3.0) { vi = -fabs(vi) * CC; yi = bx[3] - DL * 3.0; }
+    if (xi < bx[0] + DL * 3.0) { ui = fabs(ui) * CC; xi = bx[0] + DL * 3.0; }
+    if (xi > bx[1] - DL * 3.0) { ui = -fabs(ui) * CC; xi = bx[1] - DL * 3.0; }
     double zi = 0.0;
     if (DIM == 3) {
         double wi = wn[I];
         zi = z[I] + wn[I] * DT;
-        if (zi < B.zmin + DL * 3.0) { wi = fabs(wi) * CC; zi = B.zmin + DL * 3.0; }
-        if (zi > B.zmax - DL * 3.0) { wi = -fabs(wi) * CC; zi = B.zmax - DL * 3.0; }
+        if (zi < bx[4] + DL * 3.0) { wi = fabs(wi) * CC; zi = bx[4] + DL * 3.0; }
+        if (zi > bx[5] - DL * 3.0) { wi = -fabs(wi) * CC; zi = bx[5] - DL * 3.0; }
         z[I] = zi;
         wn[I] = wi;
     }
@@ -633,9 +648,11 @@ __global__ void k_commit(int n, Box B, const int* __restrict__ ptype,
         if (DIM == 3) { wI = wn[I]; w[I] = wI; }
     }
     bool bad = pI * 0 != 0 || uI * 0 != 0 || vI * 0 != 0 || (DIM == 3 && wI * 0 != 0);
+    double bx[6];
+    box_of(B, I, bx);
     double xi = x[I], yi = y[I];
-    bool out = xi >= B.xmax || yi >= B.ymax || xi <= B.xmin || yi <= B.ymin;
-    if (DIM == 3) out = out || z[I] >= B.zmax || z[I] <= B.zmin;
+    bool out = xi >= bx[1] || yi >= bx[3] || xi <= bx[0] || yi <= bx[2];
+    if (DIM == 3) out = out || z[I] >= bx[5] || z[I] <= bx[4];
     if (bad) set_error(err, MPS_ERR_NAN);
     if (out) set_error(err, MPS_ERR_BOX);
 }
@@ -664,7 +681,8 @@ Phys phys(mps_ctx* c)
 Box box(mps_ctx* c)
 {
     const mps_config& f = c->cfg;
-    Box B{f.xmin, f.xmax, f.ymin, f.ymax, f.zmin, f.zmax, f.l0, f.dt, f.velcor};
+    Box B{f.xmin, f.xmax, f.ymin, f.ymax, f.zmin, f.zmax, f.l0, f.dt, f.velcor,
+          c->nscenes > 1 ? c->scene : nullptr, c->sbox};
     return B;
 }
 
