@@ -224,7 +224,6 @@ def run_ours(args):
     if scenes is not None:
         s.set_scenes(*scenes)
     s.init()
-    s.set_profile(True)
     stream = torch.cuda.ExternalStream(s.stream())
 
     def barrier():
@@ -239,12 +238,12 @@ def run_ours(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         return float(t.item())
 
+    s.set_profile(False)
+    s.set_graph(bool(args.graph))
     for _ in range(args.warmup):
         s.step()
-    # ---- device-resident timed region ----
-    s.set_profile(True)
-    iters, ppe_ms = [], []
-    stage = {k: [] for k in ("ms_neighbors", "ms_explicit", "ms_ppe", "ms_post")}
+    # ---- device-resident timed region (graph mode: one launch per step) ----
+    iters = []
     sampler = ClockSampler(dev)
     barrier()
     sampler.start()
@@ -255,19 +254,33 @@ def run_ours(args):
     for _ in range(args.steps):
         status |= s.step()
         iters.append(s.scalar("cg_iters"))
-        ppe_ms.append(s.scalar("ms_ppe"))
-        for k in stage:
-            stage[k].append(s.scalar(k))
     e1.record(stream)
     barrier()
     launches = int(s.scalar("launches") - l0)
     clocks = sampler.stop()
     el_ms = max_over_ranks(e0.elapsed_time(e1))
+    relres = s.scalar("cg_relres")
+    # ---- the same steps again with CUDA events around every stage and
+    # every SpMV launch (eager launches; events cannot sit inside the graph's
+    # while node): per-kernel durations for the roofline ----
+    s.set_profile(True)
+    ppe_ms = []
+    stage = {k: [] for k in ("ms_neighbors", "ms_explicit", "ms_ppe", "ms_post")}
+    barrier()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for _ in range(args.steps):
+        status |= s.step()
+        ppe_ms.append(s.scalar("ms_ppe"))
+        for k in stage:
+            stage[k].append(s.scalar(k))
+    p1.record(stream)
+    barrier()
+    prof_ms = max_over_ranks(p0.elapsed_time(p1))
     spmv_ms = s.scalar("spmv_ms")
     spmv_n = s.scalar("spmv_launches")
     nnz_a = s.scalar("nnz_a")
     rows = float((s.get("bcon") == 0).sum())
-    relres = s.scalar("cg_relres")
     # ---- end-to-end through the API with host buffers ----
     names = ["x", "y", "z", "u", "v", "w", "p"]
     host = {k: torch.from_numpy(s.get(k)).pin_memory() for k in names}
@@ -306,6 +319,7 @@ def run_ours(args):
                        "parallelism": f"{ws} independent scenes" if ws > 1 else "1 scene",
                        "l2": "working set (lists, matrix) > 126 MB L2; no flush needed"},
             "fluid_particle_steps_per_s": fp * args.steps * ws / (el_ms * 1e-3),
+            "graph": bool(args.graph), "ms_per_step_profiled_eager": prof_ms / args.steps,
             "ppe_ms_per_step": statistics.mean(ppe_ms), "cg_iters_mean": statistics.mean(iters),
             "cg_relres_last": relres, "status_bits": status,
             "stage_ms": {k[3:]: statistics.mean(v) for k, v in stage.items()},
@@ -314,7 +328,9 @@ def run_ours(args):
                          "frac": (achieved / peak) if achieved else None,
                          "traffic": traffic, "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": algo,
-                         "avg_launch_ms": spmv_avg_ms, "launches_timed": int(spmv_n)},
+                         "avg_launch_ms": spmv_avg_ms, "launches_timed": int(spmv_n),
+                         "duration_source": "CUDA events around every k_cg_spmv launch "
+                                            "over the K profiled steps"},
             "e2e": {"value": n * args.steps * ws / (e2e_ms * 1e-3), "unit": METRIC,
                     "h2d_bytes_per_step": bytes_state, "d2h_bytes_per_step": bytes_state},
             "gpu_launches": launches, "clocks": clocks,
@@ -335,6 +351,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--graph", type=int, default=1, choices=[0, 1],
+                    help="1: each step is one CUDA graph launch (CG loop as a while node)")
     ap.add_argument("--config", type=int, default=1, choices=[0, 1, 3, 4],
                     help="benchmark configuration (1: the headline 3D dam break)")
     ap.add_argument("--scale", type=int, default=0,

@@ -152,6 +152,14 @@ int mps_get_state(mps_ctx* ctx, double* x, double* y, double* z, double* u, doub
  * scalars ms_neighbors ms_explicit ms_ppe ms_post ms_step (last step) and
  * spmv_ms / spmv_launches, lists_ms (accumulated) are available. */
 int mps_set_profile(mps_ctx* ctx, int on);
+
+/* Graph mode (no reference counterpart; the reference launches every stage
+ * from the host).  When on, mps_step captures the whole step, the PPE's CG
+ * loop included as a conditional while node, into a CUDA graph on its first
+ * call for each of the two reorder buffer sets and replays it afterwards:
+ * one graph launch and one host synchronisation per step.  Results are
+ * identical to eager mode.  Off while profiling (mps_set_profile). */
+int mps_set_graph(mps_ctx* ctx, int on);
 /* Scalars: n0_s n0_l lambda_l cg_iters cg_relres n nnz_s nnz_l nnz_a steps
  * cap_s cap_l len_max_s len_max_l launches pmax and the profile timings. */
 int mps_get_scalar(mps_ctx* ctx, const char* name, double* out);

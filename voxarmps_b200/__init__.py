@@ -44,7 +44,7 @@ EXPORTS = [
     "mps_integrate", "mps_collision", "mps_commit", "mps_step", "mps_run", "mps_download",
     "mps_download_lists", "mps_get_scalar", "mps_get_error", "mps_last_message",
     "mps_write_vtu", "mps_stream", "mps_set_state", "mps_get_state", "mps_set_profile",
-    "mps_cell_order_noalloc", "mps_set_scenes",
+    "mps_cell_order_noalloc", "mps_set_scenes", "mps_set_graph",
 ]
 
 _LIB = None
@@ -89,6 +89,7 @@ def load_library(path: str = LIB_PATH):
     lib.mps_set_state.argtypes = [P, P, P, P, P, P, P, P]
     lib.mps_get_state.argtypes = [P, P, P, P, P, P, P, P]
     lib.mps_set_profile.argtypes = [P, C.c_int]
+    lib.mps_set_graph.argtypes = [P, C.c_int]
     lib.mps_set_scenes.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
                                    C.POINTER(C.c_double)]
     lib.mps_cell_order_noalloc.argtypes = [C.POINTER(MpsConfig), C.c_double, C.c_int, P, P, P,
@@ -239,6 +240,10 @@ class Solver:
 
     def set_profile(self, on: bool = True):
         return self._chk(self.lib.mps_set_profile(self.h, int(on)), "profile")
+
+    def set_graph(self, on: bool = True):
+        """Replay each step as one CUDA graph (CG loop as a while node)."""
+        return self._chk(self.lib.mps_set_graph(self.h, int(on)), "graph")
 
     def scalar(self, name: str) -> float:
         v = C.c_double()

@@ -56,10 +56,22 @@ int halloc(mps_ctx* c, T** p, size_t count)
     return MPS_OK;
 }
 
+// Step graphs hold the buffer addresses they were captured with.
+void drop_graphs(mps_ctx* c)
+{
+    for (int k = 0; k < 2; k++) {
+        if (c->gexec[k]) cudaGraphExecDestroy(c->gexec[k]);
+        c->gexec[k] = nullptr;
+        c->gkernels[k] = 0;
+    }
+}
+
 void free_all(mps_ctx* c)
 {
     if (c->device >= 0) cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graphs(c);
+    c->swaps = 0;
     for (void* q : c->owned) cudaFree(q);
     for (void* q : c->pinned) cudaFreeHost(q);
     c->owned.clear();
@@ -312,6 +324,7 @@ int mps_destroy(mps_ctx* c)
         if (e) cudaEventDestroy(e);
     for (auto& e : c->ev_spmv) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->stream2) cudaStreamDestroy(c->stream2);
     delete c;
     return MPS_OK;
 }
@@ -412,6 +425,7 @@ int mps_set_scenes(mps_ctx* c, int nscenes, const int* scene, const double* boxe
     for (int i = 0; i < c->n; i++)
         if (scene[i] < 0 || scene[i] >= nscenes) return MPS_ERR_ARG;
     VMPS_CUDA(c, cudaSetDevice(c->device));
+    drop_graphs(c);
     c->nscenes = nscenes;
     TRY(dalloc(c, &c->sbox, (size_t)6 * nscenes));
     TRY(dalloc(c, &c->spmax, (size_t)nscenes));
@@ -470,6 +484,7 @@ int mps_init(mps_ctx* c)
 {
     if (!c || c->n == 0) return MPS_ERR_ARG;
     VMPS_CUDA(c, cudaSetDevice(c->device));
+    drop_graphs(c);
     TRY(vmps_neighbors(c));
     VMPS_CUDA(c, cudaMemsetAsync(c->d_max, 0, sizeof(unsigned long long), c->stream));
     TRY(vmps_pnd(c, 0, 1, 1, c->nd));
@@ -522,18 +537,19 @@ int mps_pressure(mps_ctx* c, int* iters, double* relres)
         c->cg_relres = 0;
     } else {
         TRY(vmps_ppe(c));
+        VMPS_CUDA(c, cudaStreamSynchronize(c->stream));
+        TRY(vmps_ppe_finish(c));
     }
     if (iters) *iters = c->cg_iters;
     if (relres) *relres = c->cg_relres;
     return MPS_OK;
 }
 
-int mps_step(mps_ctx* c)
+// The stage sequence of one loop iteration (main.cu:1036-1337), enqueued
+// on the context's stream without host synchronisation in graph mode.
+static int enqueue_step(mps_ctx* c)
 {
-    NEED_INIT(c);
-    VMPS_CUDA(c, cudaSetDevice(c->device));
     const mps_config& f = c->cfg;
-    unsigned int before = c->host_err;
     auto mark = [&](int k) -> int {
         if (c->profile) VMPS_CUDA(c, cudaEventRecord(c->ev[k], c->stream));
         return MPS_OK;
@@ -558,8 +574,55 @@ int mps_step(mps_ctx* c)
     TRY(vmps_collision(c));
     TRY(vmps_commit(c));
     TRY(mark(4));
+    return MPS_OK;
+}
+
+// One step as a CUDA graph.  The reorder alternates the persistent fields
+// between two buffer sets, so a graph is captured per buffer parity and
+// replayed afterwards; the CG loop inside is a conditional while node.
+static int graph_step(mps_ctx* c)
+{
+    const int par = (int)(c->swaps & 1);
+    if (!c->stream2) VMPS_CUDA(c, cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
+    if (!c->gexec[par]) {
+        const long long l0 = g_launches.load();
+        VMPS_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+        int r = enqueue_step(c);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (r != MPS_OK || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            if (r != MPS_OK) return r;
+            VMPS_CUDA(c, e);
+        }
+        cudaError_t ie = cudaGraphInstantiate(&c->gexec[par], g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) c->gexec[par] = nullptr;
+        VMPS_CUDA(c, ie);
+        c->gkernels[par] = (long)(g_launches.load() - l0);
+    } else {
+        // the host side of a replay: the reorder's buffer exchange
+        vmps_reorder_swap(c);
+        vmps_count_launch((int)c->gkernels[par]);
+        c->ppe_pending = c->cfg.method != 3;
+    }
+    VMPS_CUDA(c, cudaGraphLaunch(c->gexec[par], c->stream));
+    return MPS_OK;
+}
+
+int mps_step(mps_ctx* c)
+{
+    NEED_INIT(c);
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    unsigned int before = c->host_err;
+    const bool graph = c->use_graph && !c->profile;
+    if (graph) TRY(graph_step(c));
+    else TRY(enqueue_step(c));
     c->steps++;
     int e = collect_errors(c);
+    TRY(vmps_ppe_finish(c));
+    if (graph && c->cfg.method != 3) vmps_count_launch(c->cg_iters * c->cg_loop_kernels);
     if (c->profile) {
         for (int k = 0; k < 4; k++) {
             float ms = 0;
@@ -571,6 +634,15 @@ int mps_step(mps_ctx* c)
         c->ms_stage[4] = ms;
     }
     return e | (int)(c->host_err & ~before);
+}
+
+int mps_set_graph(mps_ctx* c, int on)
+{
+    if (!c) return MPS_ERR_ARG;
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    if (!on) drop_graphs(c);
+    c->use_graph = on != 0;
+    return MPS_OK;
 }
 
 int mps_run(mps_ctx* c, int steps)

@@ -85,6 +85,7 @@ struct mps_ctx {
     mps_config cfg;
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;   // captures the CG loop body into its while node
     std::string msg;
     int n = 0, pitch = 0;
     int gp = 0, wp = 0, fp = 0;
@@ -93,6 +94,14 @@ struct mps_ctx {
     int cap_l = 0, cap_s = 0;
     double n0_s = 0, n0_l = 0, lambda_l = 0;
     int cg_iters = 0;
+    int cg_loop_kernels = 4, cg_nspmv = 0;
+    bool ppe_pending = false;
+    // CUDA graph of one step per buffer parity (the reorder double-buffers
+    // the persistent state, so the step's pointers alternate with period 2)
+    bool use_graph = false;
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    long gkernels[2] = {0, 0};
+    long swaps = 0;
     double cg_relres = 0;
     long steps = 0;
     bool initialized = false;
@@ -336,6 +345,8 @@ int vmps_predict(mps_ctx* ctx);
 int vmps_bcon(mps_ctx* ctx);
 int vmps_pressure_wc(mps_ctx* ctx);
 int vmps_ppe(mps_ctx* ctx);
+int vmps_ppe_finish(mps_ctx* ctx);
+void vmps_reorder_swap(mps_ctx* ctx);
 int vmps_phat(mps_ctx* ctx);
 int vmps_pressgrad(mps_ctx* ctx);
 int vmps_integrate(mps_ctx* ctx);

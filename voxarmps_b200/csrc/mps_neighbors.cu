@@ -353,6 +353,23 @@ static void persistent_set(mps_ctx* ctx, GatherSet& g, std::vector<void**>& slot
 // they are registered by vmps_alloc_reorder() in mps_context.cu.
 extern std::vector<void*>& vmps_reorder_alts(mps_ctx* ctx);
 
+// Exchange the persistent fields with their alternates (the reorder wrote
+// the alternates).  A replayed step graph skips the capture-time host code,
+// so the graph path calls this once per replay.
+void vmps_reorder_swap(mps_ctx* ctx)
+{
+    GatherSet g;
+    std::vector<void**> slots;
+    std::vector<void*>& alts = vmps_reorder_alts(ctx);
+    persistent_set(ctx, g, slots, alts);
+    for (int a = 0; a < g.count; a++) {
+        void* old = *slots[a];
+        *slots[a] = alts[a];
+        alts[a] = old;
+    }
+    ctx->swaps++;
+}
+
 int vmps_neighbors(mps_ctx* ctx)
 {
     const int n = ctx->n;
@@ -386,11 +403,7 @@ int vmps_neighbors(mps_ctx* ctx)
     persistent_set(ctx, g, slots, alts);
     k_gather<<<nb, kBlock, 0, st>>>(n, ctx->src, g);
     vmps_count_launch(1);
-    for (int a = 0; a < g.count; a++) {
-        void* old = *slots[a];
-        *slots[a] = alts[a];
-        alts[a] = old;
-    }
+    vmps_reorder_swap(ctx);
     k_translate<<<nb, kBlock, 0, st>>>(n, ctx->inv, ctx->perm_s_tmp, ctx->perm_s);
     vmps_count_launch(1);
     if (ctx->nscenes > 1) {

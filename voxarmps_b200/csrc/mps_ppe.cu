@@ -19,7 +19,7 @@ using namespace vmps;
 
 namespace {
 
-enum { S_BB = 0, S_RZ, S_RR, S_ZERO, S_NEWRZ, S_NEWRR, S_DONE, S_COUNT };
+enum { S_BB = 0, S_RZ, S_RR, S_ZERO, S_NEWRZ, S_NEWRR, S_DONE, S_WORST, S_COUNT };
 constexpr int kRedThreads = 256;
 
 __device__ __forceinline__ double block_sum(double v, double* sh)
@@ -261,7 +261,8 @@ __global__ void k_cg_start(CG A, const double* __restrict__ b, const double* __r
 }
 
 __global__ void k_cg_start_scalars(int nparts, const double* __restrict__ part, double tol2,
-                                   double* scal, int* flag)
+                                   double* scal, int* flag, int use_cond,
+                                   cudaGraphConditionalHandle cond)
 {
     __shared__ double sh[33];
     double bb = reduce_parts(part, nparts, sh);
@@ -274,6 +275,8 @@ __global__ void k_cg_start_scalars(int nparts, const double* __restrict__ part, 
         scal[S_ZERO] = (bb == 0.0) ? 1.0 : 0.0;
         flag[0] = (bb == 0.0 || rr <= tol2 * bb) ? 1 : 0;
         flag[1] = 0;
+        // inside a CUDA graph the CG loop is a while node on this value
+        if (use_cond) cudaGraphSetConditional(cond, flag[0] ? 0u : 1u);
     }
 }
 
@@ -393,13 +396,29 @@ __global__ void k_invert(int n, const int* __restrict__ oid, int* __restrict__ i
     if (i < n) inv_id[oid[i]] = i;
 }
 
-__global__ void k_cg_commit(double* scal, int* flag)
+// commits the iteration; inside a graph it also sets the while-node
+// condition (the iteration cap in k_cg_direction bounds the loop)
+__global__ void k_cg_commit(double* scal, int* flag, int use_cond,
+                            cudaGraphConditionalHandle cond)
 {
-    if (flag[0]) return;
-    scal[S_RZ] = scal[S_NEWRZ];
-    scal[S_RR] = scal[S_NEWRR];
-    flag[1] += 1;
-    if (scal[S_DONE] != 0.0) flag[0] = 1;
+    if (!flag[0]) {
+        scal[S_RZ] = scal[S_NEWRZ];
+        scal[S_RR] = scal[S_NEWRR];
+        flag[1] += 1;
+        if (scal[S_DONE] != 0.0) flag[0] = 1;
+    }
+    if (use_cond) cudaGraphSetConditional(cond, flag[0] ? 0u : 1u);
+}
+
+// worst relative residual over batched scenes -> scal[S_WORST]
+__global__ void k_scene_worst(int nscenes, const double* __restrict__ sbb,
+                              const double* __restrict__ srr, double* scal)
+{
+    if (threadIdx.x != 0) return;
+    double worst = 0.0;
+    for (int k = 0; k < nscenes; k++)
+        if (sbb[k] > 0) worst = fmax(worst, sqrt(srr[k] / sbb[k]));
+    scal[S_WORST] = worst;
 }
 
 // clamp (functions.cu:2534-2547); a zero right-hand side gives p = 0
@@ -482,66 +501,118 @@ int vmps_ppe(mps_ctx* c)
     CG G{c->mcol, c->mval, c->mlen, c->moff, c->diag, c->bcon, c->cap_l, n,
          f.solver == 1 ? 1 : 0, nblk};
     double tol2 = f.cg_tol * f.cg_tol;
+    const bool batched = c->nscenes > 1;
+    // Inside a stream capture (graph mode) the loop becomes a conditional
+    // while node: no host synchronisation anywhere in the solve.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaGraph_t cgraph = nullptr;
+    VMPS_CUDA(c, cudaStreamGetCaptureInfo(st, &cap, nullptr, &cgraph, nullptr, nullptr));
+    const bool graph = cap == cudaStreamCaptureStatusActive;
+    cudaGraphConditionalHandle cond = 0;
+    if (graph) VMPS_CUDA(c, cudaGraphConditionalHandleCreate(&cond, cgraph, 1, cudaGraphCondAssignDefault));
     k_cg_start<<<nblk, kRedThreads, 0, st>>>(G, c->source, c->pnew, c->cg_r, c->cg_z, c->cg_p,
                                              c->cg_part);
-    k_cg_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal, c->cg_flag);
+    k_cg_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal, c->cg_flag,
+                                                  graph ? 1 : 0, cond);
     vmps_count_launch(2);
-    const bool batched = c->nscenes > 1;
     if (batched) {
         k_scene_sums<<<c->nscenes, kRedThreads, 0, st>>>(0, c->sfirst, c->slast, c->scene, c->bcon,
                                                          c->source, tol2, c->sbb, nullptr, nullptr,
                                                          nullptr);
         vmps_count_launch(1);
     }
-    const int check = 4;
-    int it = 0;
-    int nspmv = 0;
-    for (; it < f.cg_max; it++) {
-        if (c->profile) {
-            while ((int)c->ev_spmv.size() < 2 * (nspmv + 1)) {
+    // one CG iteration on stream s (profiling events only outside graphs)
+    auto iteration = [&](cudaStream_t s, int k) -> int {
+        if (c->profile && !graph) {
+            while ((int)c->ev_spmv.size() < 2 * (k + 1)) {
                 cudaEvent_t e;
                 VMPS_CUDA(c, cudaEventCreate(&e));
                 c->ev_spmv.push_back(e);
             }
-            VMPS_CUDA(c, cudaEventRecord(c->ev_spmv[2 * nspmv], st));
+            VMPS_CUDA(c, cudaEventRecord(c->ev_spmv[2 * k], s));
         }
-        k_cg_spmv<<<nblk, kRedThreads, 0, st>>>(G, c->cg_p, c->cg_s, c->cg_part + 4 * nblk,
-                                                c->cg_flag);
-        if (c->profile) VMPS_CUDA(c, cudaEventRecord(c->ev_spmv[2 * nspmv + 1], st));
-        nspmv++;
-        k_cg_update<<<nblk, kRedThreads, 0, st>>>(G, c->pnew, c->cg_r, c->cg_z, c->cg_p, c->cg_s,
-                                                  c->cg_part + 4 * nblk, c->cg_part, c->cg_scal,
-                                                  c->cg_flag);
-        if (batched) {
-            k_scene_sums<<<c->nscenes, kRedThreads, 0, st>>>(1, c->sfirst, c->slast, c->scene,
-                                                             c->bcon, c->cg_r, tol2, c->sbb,
-                                                             c->srr, c->sok, c->cg_flag);
-            vmps_count_launch(1);
-        }
-        k_cg_direction<<<nblk, kRedThreads, 0, st>>>(G, c->cg_z, c->cg_p, c->cg_part, c->cg_scal,
-                                                     c->cg_flag, tol2, f.cg_max, c->nscenes,
-                                                     c->sok);
-        k_cg_commit<<<1, 1, 0, st>>>(c->cg_scal, c->cg_flag);
-        vmps_count_launch(4);
-        if ((it + 1) % check == 0 || it + 1 == f.cg_max) {
-            VMPS_CUDA(c, cudaMemcpyAsync(c->cg_flag_host, c->cg_flag, 2 * sizeof(int),
-                                         cudaMemcpyDeviceToHost, st));
-            VMPS_CUDA(c, cudaStreamSynchronize(st));
-            if (c->cg_flag_host[0]) break;
+        k_cg_spmv<<<nblk, kRedThreads, 0, s>>>(G, c->cg_p, c->cg_s, c->cg_part + 4 * nblk,
+                                               c->cg_flag);
+        if (c->profile && !graph) VMPS_CUDA(c, cudaEventRecord(c->ev_spmv[2 * k + 1], s));
+        k_cg_update<<<nblk, kRedThreads, 0, s>>>(G, c->pnew, c->cg_r, c->cg_z, c->cg_p, c->cg_s,
+                                                 c->cg_part + 4 * nblk, c->cg_part, c->cg_scal,
+                                                 c->cg_flag);
+        if (batched)
+            k_scene_sums<<<c->nscenes, kRedThreads, 0, s>>>(1, c->sfirst, c->slast, c->scene,
+                                                            c->bcon, c->cg_r, tol2, c->sbb,
+                                                            c->srr, c->sok, c->cg_flag);
+        k_cg_direction<<<nblk, kRedThreads, 0, s>>>(G, c->cg_z, c->cg_p, c->cg_part, c->cg_scal,
+                                                    c->cg_flag, tol2, f.cg_max, c->nscenes,
+                                                    c->sok);
+        k_cg_commit<<<1, 1, 0, s>>>(c->cg_scal, c->cg_flag, graph ? 1 : 0, cond);
+        VMPS_CUDA(c, cudaGetLastError());
+        return MPS_OK;
+    };
+    c->cg_loop_kernels = batched ? 5 : 4;
+    c->cg_nspmv = 0;
+    if (graph) {
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        VMPS_CUDA(c, cudaStreamGetCaptureInfo(st, &cap, nullptr, &cgraph, &deps, &ndeps));
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = cond;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        VMPS_CUDA(c, cudaGraphAddNode(&node, cgraph, deps, ndeps, &np));
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        VMPS_CUDA(c, cudaStreamUpdateCaptureDependencies(st, &node, 1,
+                                                         cudaStreamSetCaptureDependencies));
+        if (!c->stream2)
+            VMPS_CUDA(c, cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
+        VMPS_CUDA(c, cudaStreamBeginCaptureToGraph(c->stream2, body, nullptr, nullptr, 0,
+                                                   cudaStreamCaptureModeRelaxed));
+        int r = iteration(c->stream2, 0);
+        cudaGraph_t done_body = nullptr;
+        VMPS_CUDA(c, cudaStreamEndCapture(c->stream2, &done_body));
+        if (r != MPS_OK) return r;
+    } else {
+        const int check = 4;
+        for (int it = 0; it < f.cg_max; it++) {
+            int r = iteration(st, it);
+            if (r != MPS_OK) return r;
+            vmps_count_launch(c->cg_loop_kernels);
+            c->cg_nspmv++;
+            if ((it + 1) % check == 0 || it + 1 == f.cg_max) {
+                VMPS_CUDA(c, cudaMemcpyAsync(c->cg_flag_host, c->cg_flag, 2 * sizeof(int),
+                                             cudaMemcpyDeviceToHost, st));
+                VMPS_CUDA(c, cudaStreamSynchronize(st));
+                if (c->cg_flag_host[0]) break;
+            }
         }
     }
+    if (batched) {
+        k_scene_worst<<<1, 32, 0, st>>>(c->nscenes, c->sbb, c->srr, c->cg_scal);
+        vmps_count_launch(1);
+    }
+    k_clamp<<<grid_blocks(n), kBlock, 0, st>>>(n, f.pmin, f.pmax, c->cg_scal, c->pnew,
+                                               batched ? c->scene : nullptr, c->spmax, c->sbb);
+    vmps_count_launch(1);
     VMPS_CUDA(c, cudaMemcpyAsync(c->cg_flag_host, c->cg_flag, 2 * sizeof(int),
                                  cudaMemcpyDeviceToHost, st));
     VMPS_CUDA(c, cudaMemcpyAsync(c->red_host, c->cg_scal, S_COUNT * sizeof(double),
                                  cudaMemcpyDeviceToHost, st));
-    k_clamp<<<grid_blocks(n), kBlock, 0, st>>>(n, f.pmin, f.pmax, c->cg_scal, c->pnew,
-                                               batched ? c->scene : nullptr, c->spmax, c->sbb);
-    vmps_count_launch(1);
-    VMPS_CUDA(c, cudaStreamSynchronize(st));
+    VMPS_CUDA(c, cudaGetLastError());
+    c->ppe_pending = true;
+    return MPS_OK;
+}
+
+// After the stream has been synchronised: iteration count, residual, status.
+int vmps_ppe_finish(mps_ctx* c)
+{
+    if (!c->ppe_pending) return MPS_OK;
+    c->ppe_pending = false;
+    const mps_config& f = c->cfg;
     c->cg_iters = c->cg_flag_host[1];
     if (c->profile) {
-        // spmv launches after convergence exit at once: count the working ones
-        for (int k = 0; k < nspmv && k < c->cg_iters; k++) {
+        // launches after convergence exit at once: count the working ones
+        for (int k = 0; k < c->cg_nspmv && k < c->cg_iters; k++) {
             float ms = 0;
             VMPS_CUDA(c, cudaEventElapsedTime(&ms, c->ev_spmv[2 * k], c->ev_spmv[2 * k + 1]));
             c->spmv_ms += ms;
@@ -550,17 +621,7 @@ int vmps_ppe(mps_ctx* c)
     }
     double bb = c->red_host[S_BB], rr = c->red_host[S_RR];
     c->cg_relres = bb > 0 ? sqrt(rr / bb) : 0.0;
-    if (batched) {  // the worst scene's relative residual
-        std::vector<double> hb(c->nscenes), hr(c->nscenes);
-        VMPS_CUDA(c, cudaMemcpy(hb.data(), c->sbb, sizeof(double) * c->nscenes,
-                                cudaMemcpyDeviceToHost));
-        VMPS_CUDA(c, cudaMemcpy(hr.data(), c->srr, sizeof(double) * c->nscenes,
-                                cudaMemcpyDeviceToHost));
-        double worst = 0.0;
-        for (int k = 0; k < c->nscenes; k++)
-            if (hb[k] > 0) worst = std::max(worst, sqrt(hr[k] / hb[k]));
-        c->cg_relres = worst;
-    }
+    if (c->nscenes > 1) c->cg_relres = c->red_host[S_WORST];
     if (!(c->cg_relres <= f.cg_tol)) c->host_err |= MPS_ERR_NOT_CONVERGED;
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;

@@ -568,63 +568,87 @@ struct CollArgs {
 
 // COLLISION2 (functions.cu:1523-1601) in its order-independent form: each
 // fluid particle gathers the impulse of every approaching pair (d < coll)
-// from the pre-collision state.  Writes the new state to the *o arrays.
+// from the pre-collision state.  The position and velocity changes go to the
+// delta arrays; k_collision_apply adds them once every particle has read the
+// pre-collision state (no buffer swap, so the step's buffers stay fixed).
 template <int DIM, int G>
 __global__ void k_collision(int n, Lists L, CollArgs A, const int* __restrict__ ptype,
                             const double4* __restrict__ P4, const double* __restrict__ un,
                             const double* __restrict__ vn, const double* __restrict__ wn,
-                            double* __restrict__ xo, double* __restrict__ yo,
-                            double* __restrict__ zo, double* __restrict__ uo,
-                            double* __restrict__ vo, double* __restrict__ wo,
-                            double4* __restrict__ P4o)
+                            double* __restrict__ dxo, double* __restrict__ dyo,
+                            double* __restrict__ dzo, double* __restrict__ duo,
+                            double* __restrict__ dvo, double* __restrict__ dwo)
 {
     Grp<G> q;
     int i = (int)q.gid;
     if (i >= n) return;
+    int pti = ptype[i];
+    if (pti <= 0) return;
     double4 pi = P4[i];
     double ui = un[i], vi = vn[i], wi = DIM == 3 ? wn[i] : 0.0;
-    int pti = ptype[i];
     double du = 0, dv = 0, dw = 0, ddx = 0, ddy = 0, ddz = 0;
-    if (pti > 0) {
-        double m1 = (pti == 1) ? A.rho1 : A.rho2;
-        const int* row = row_of(L, i);
-        int len = L.len[i];
-        for (int k = q.lane; k < len; k += G) {
-            int j = row[k];
-            if (i == j) continue;
-            double ex, ey, ez;
-            double d2 = d2of<DIM>(pi, P4[j], ex, ey, ez);
-            if (!(d2 < A.coll2)) continue;
-            double d = sqrt(d2);
-            double m2 = (ptype[j] == 1) ? A.rho1 : A.rho2;
-            double ug = (m1 * ui + m2 * un[j]) / (m1 + m2);
-            double vg = (m1 * vi + m2 * vn[j]) / (m1 + m2);
-            double ur = m1 * (ui - ug), vr = m1 * (vi - vg), vabs;
-            if (DIM == 3) {
-                double wg = (m1 * wi + m2 * wn[j]) / (m1 + m2);
-                double wr = m1 * (wi - wg);
-                vabs = (ur * ex + vr * ey + wr * ez) / d;
-            } else {
-                vabs = (ur * ex + vr * ey) / d;
-            }
-            if (!(vabs > 0)) continue;
-            double um = (1.0 + A.cc) * vabs * ex / d;
-            double vm = (1.0 + A.cc) * vabs * ey / d;
-            du -= um / m1; dv -= vm / m1;
-            ddx -= A.dt * um / m1; ddy -= A.dt * vm / m1;
-            if (DIM == 3) {
-                double wm = (1.0 + A.cc) * vabs * ez / d;
-                dw -= wm / m1; ddz -= A.dt * wm / m1;
-            }
+    double m1 = (pti == 1) ? A.rho1 : A.rho2;
+    const int* row = row_of(L, i);
+    int len = L.len[i];
+    for (int k = q.lane; k < len; k += G) {
+        int j = row[k];
+        if (i == j) continue;
+        double ex, ey, ez;
+        double d2 = d2of<DIM>(pi, P4[j], ex, ey, ez);
+        if (!(d2 < A.coll2)) continue;
+        double d = sqrt(d2);
+        double m2 = (ptype[j] == 1) ? A.rho1 : A.rho2;
+        double ug = (m1 * ui + m2 * un[j]) / (m1 + m2);
+        double vg = (m1 * vi + m2 * vn[j]) / (m1 + m2);
+        double ur = m1 * (ui - ug), vr = m1 * (vi - vg), vabs;
+        if (DIM == 3) {
+            double wg = (m1 * wi + m2 * wn[j]) / (m1 + m2);
+            double wr = m1 * (wi - wg);
+            vabs = (ur * ex + vr * ey + wr * ez) / d;
+        } else {
+            vabs = (ur * ex + vr * ey) / d;
         }
-        du = q.sum(du); dv = q.sum(dv); ddx = q.sum(ddx); ddy = q.sum(ddy);
-        if (DIM == 3) { dw = q.sum(dw); ddz = q.sum(ddz); }
+        if (!(vabs > 0)) continue;
+        double um = (1.0 + A.cc) * vabs * ex / d;
+        double vm = (1.0 + A.cc) * vabs * ey / d;
+        du -= um / m1; dv -= vm / m1;
+        ddx -= A.dt * um / m1; ddy -= A.dt * vm / m1;
+        if (DIM == 3) {
+            double wm = (1.0 + A.cc) * vabs * ez / d;
+            dw -= wm / m1; ddz -= A.dt * wm / m1;
+        }
     }
+    du = q.sum(du); dv = q.sum(dv); ddx = q.sum(ddx); ddy = q.sum(ddy);
+    if (DIM == 3) { dw = q.sum(dw); ddz = q.sum(ddz); }
     if (q.lane != 0) return;
-    double4 o = make_double4(pi.x + ddx, pi.y + ddy, DIM == 3 ? pi.z + ddz : pi.z, pi.w);
-    xo[i] = o.x; yo[i] = o.y; uo[i] = ui + du; vo[i] = vi + dv;
-    if (DIM == 3) { zo[i] = o.z; wo[i] = wi + dw; }
-    P4o[i] = o;
+    dxo[i] = ddx; dyo[i] = ddy; duo[i] = du; dvo[i] = dv;
+    if (DIM == 3) { dzo[i] = ddz; dwo[i] = dw; }
+}
+
+template <int DIM>
+__global__ void k_collision_apply(int n, const int* __restrict__ ptype, double* __restrict__ x,
+                                  double* __restrict__ y, double* __restrict__ z,
+                                  double* __restrict__ un, double* __restrict__ vn,
+                                  double* __restrict__ wn, const double* __restrict__ dx,
+                                  const double* __restrict__ dy, const double* __restrict__ dz,
+                                  const double* __restrict__ du, const double* __restrict__ dv,
+                                  const double* __restrict__ dw, double4* __restrict__ P4)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || ptype[i] <= 0) return;
+    double4 pi = P4[i];
+    pi.x = pi.x + dx[i];
+    pi.y = pi.y + dy[i];
+    x[i] = pi.x;
+    y[i] = pi.y;
+    un[i] = un[i] + du[i];
+    vn[i] = vn[i] + dv[i];
+    if (DIM == 3) {
+        pi.z = pi.z + dz[i];
+        z[i] = pi.z;
+        wn[i] = wn[i] + dw[i];
+    }
+    P4[i] = pi;
 }
 
 // PREPDATA (functions.cu:2688-2746): roll state, flag ERROR#1 / ERROR#2
@@ -862,19 +886,12 @@ int vmps_collision(mps_ctx* c)
 {
     const mps_config& f = c->cfg;
     CollArgs A{sqrt_cut(f.coll, true), f.cc, f.dt, f.rho1, f.rho2};
-    // the new state goes to the *c buffers, which then swap roles with it
+    // deltas to the *c scratch arrays, then applied in place
     LAUNCH_SMALL(k_collision, c->n, lists(c, 1), A, c->ptype, c->P4, c->un, c->vn, c->wn, c->xc,
-               c->yc, c->zc, c->uc, c->vc, c->wc, c->P4c);
+                 c->yc, c->zc, c->uc, c->vc, c->wc);
+    LAUNCH_DIM(k_collision_apply, c->n, c->ptype, c->x, c->y, c->z, c->un, c->vn, c->wn, c->xc,
+               c->yc, c->zc, c->uc, c->vc, c->wc, c->P4);
     VMPS_CUDA(c, cudaGetLastError());
-    std::swap(c->x, c->xc);
-    std::swap(c->y, c->yc);
-    std::swap(c->un, c->uc);
-    std::swap(c->vn, c->vc);
-    std::swap(c->P4, c->P4c);
-    if (c->cfg.dim == 3) {
-        std::swap(c->z, c->zc);
-        std::swap(c->wn, c->wc);
-    }
     return MPS_OK;
 }
 
