@@ -110,10 +110,24 @@ class ClockSampler:
 
 
 def spmv_algorithmic_bytes(nnz_a: float, rows: float) -> float:
-    """Bytes one FP64 ELL SpMV must move: per stored non-zero a column index
-    (4 B) and a value (8 B); per unknown row diag (8), length (4), bcon (4),
-    the row's own p (8) and the written s (8).  Gathers of p_j are L2 hits."""
-    return nnz_a * 12.0 + rows * 32.0
+    """Bytes one FP64 CSR SpMV must move: per stored non-zero a column index
+    (4 B) and a value (8 B); per unknown row diag (8), length (4), offset (4),
+    bcon (4), the row's own p (8) and the written s (8).  Gathers of p_j are
+    L2 hits."""
+    return nnz_a * 12.0 + rows * 36.0
+
+
+def spmv32_algorithmic_bytes(nnz_a: float, rows: float) -> float:
+    """Inner SpMV of the mixed-precision PPE: column index (4 B) and FP32
+    value (4 B) per non-zero; per row diag (8), length, offset, bcon (4 each),
+    FP32 p and s (4 each)."""
+    return nnz_a * 8.0 + rows * 28.0
+
+
+def refine_algorithmic_bytes(nnz_a: float, rows: float) -> float:
+    """Refinement r -= A64 d, x += d: 12 B per non-zero; per row diag (8),
+    length, offset, bcon, FP32 d (4 each), r and x read and written (32)."""
+    return nnz_a * 12.0 + rows * 56.0
 
 
 WORKLOADS = {
@@ -121,6 +135,9 @@ WORKLOADS = {
        "re=2.1/4.0*l0, dt=1e-4, FP64 Jacobi-PCG to 1e-8",
     1: "3D dam break, 80x160x80 fluid (1,024,000) + 571,308 wall/dummy particles, l0=0.005, "
        "re=2.1/4.0*l0, dt=5e-5, FP64 Jacobi-PCG to 1e-8 relative residual",
+    2: "3D dam break, 80x160x80 fluid (1,024,000) + 571,308 wall/dummy particles, l0=0.005, "
+       "re=2.1/4.0*l0, dt=5e-5, mixed-precision PPE (FP32 inner CG, FP64 dots and "
+       "refinement) to 1e-8 relative residual",
     3: "2D two-phase dam, water 600x100 + Bingham block 150x150 (82,500 fluid), l0=0.002, "
        "SPS-LES Cs=0.12, HB second fluid, dt=1e-4, FP64 Jacobi-PCG to 1e-8",
     4: "64 batched 2D dam breaks (splitmix64 seed 0, columns U[0.1,0.4]x U[0.2,0.6] m, "
@@ -128,7 +145,7 @@ WORKLOADS = {
 }
 
 
-def build_case(scale: int = 0, which: int = 1):
+def build_case(scale: int = 0, which: int = 1, precision=None):
     """(cfg, case, scenes) of the benchmark scene; scale > 0 selects the
     smaller 3D dam used for profiling captures (config.scaled_dam3d)."""
     from voxarmps_b200 import config
@@ -144,6 +161,8 @@ def build_case(scale: int = 0, which: int = 1):
     cfg = config.solver_semantics(cfg)
     cfg["cg_tol"] = 1e-8
     cfg["cg_max"] = 1000
+    # configs 2 and 4 name the mixed-precision PPE
+    cfg["precision"] = (1 if which in (2, 4) else 0) if precision is None else precision
     return cfg, case, scenes
 
 
@@ -217,7 +236,8 @@ def run_ours(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    cfg, case, scenes = build_case(args.scale, args.config)
+    cfg, case, scenes = build_case(args.scale, args.config, args.precision)
+    mixed = cfg["precision"] == 1
     n = len(case["x"])
     fp = int((case["ptype"] > 0).sum())
     s = vm.Solver(cfg, case, device=dev)
@@ -264,7 +284,7 @@ def run_ours(args):
     # every SpMV launch (eager launches; events cannot sit inside the graph's
     # while node): per-kernel durations for the roofline ----
     s.set_profile(True)
-    ppe_ms = []
+    ppe_ms, inner, outer = [], 0, 0
     stage = {k: [] for k in ("ms_neighbors", "ms_explicit", "ms_ppe", "ms_post")}
     barrier()
     p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -272,6 +292,8 @@ def run_ours(args):
     for _ in range(args.steps):
         status |= s.step()
         ppe_ms.append(s.scalar("ms_ppe"))
+        inner += s.scalar("cg_iters")
+        outer += s.scalar("cg_outer")
         for k in stage:
             stage[k].append(s.scalar(k))
     p1.record(stream)
@@ -301,18 +323,25 @@ def run_ours(args):
     bytes_state = 8 * n * len(names)
     peak, peak_kind = peaks()
     spmv_avg_ms = spmv_ms / max(spmv_n, 1)
-    algo = spmv_algorithmic_bytes(nnz_a, rows)
+    if mixed:  # launches of k_ir_spmv: inner FP32 SpMVs and FP64 refinements
+        algo = (inner * spmv32_algorithmic_bytes(nnz_a, rows) +
+                outer * refine_algorithmic_bytes(nnz_a, rows)) / max(inner + outer, 1)
+    else:
+        algo = spmv_algorithmic_bytes(nnz_a, rows)
     achieved = algo / (spmv_avg_ms * 1e-3) / 1e9 if spmv_n else None
-    traffic = SPMV_TRAFFIC_OVER_ALGORITHMIC * algo
+    # DRAM bytes per launch from the ncu capture of the FP64 SpMV (scaled by
+    # its traffic/algorithmic ratio); not captured for the mixed kernel
+    traffic = None if mixed else SPMV_TRAFFIC_OVER_ALGORITHMIC * algo
     line = None
     if rank == 0:
         cpu = (time_reference(steps=3, warmup=1, nthreads=os.cpu_count() or 1)
-               if ws == 1 and args.config == 1 and not args.scale else None)
+               if ws == 1 and args.config in (1, 2) and not args.scale else None)
         value = n * args.steps * ws / (el_ms * 1e-3)
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": el_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64",
+            "data": "synthetic",
             "config": {"workload": (WORKLOADS[args.config] if not args.scale else
                                     f"3D dam break scaled x{args.scale} (profiling case)"),
                        "particles": n, "fluid_particles": fp,
@@ -321,9 +350,14 @@ def run_ours(args):
             "fluid_particle_steps_per_s": fp * args.steps * ws / (el_ms * 1e-3),
             "graph": bool(args.graph), "ms_per_step_profiled_eager": prof_ms / args.steps,
             "ppe_ms_per_step": statistics.mean(ppe_ms), "cg_iters_mean": statistics.mean(iters),
+            "precision": "mixed (FP32 inner CG, FP64 dots/refinement)" if mixed else "fp64",
+            "cg_outer_mean": outer / args.steps,
             "cg_relres_last": relres, "status_bits": status,
             "stage_ms": {k[3:]: statistics.mean(v) for k, v in stage.items()},
-            "roofline": {"kernel": "k_cg_spmv (PPE SpMV, FP64 CSR, warp per row)", "bound": "hbm",
+            "roofline": {"kernel": ("k_ir_spmv (mixed PPE: FP32 inner SpMV + FP64 refinement, "
+                                    "CSR, warp per row)" if mixed else
+                                    "k_cg_spmv (PPE SpMV, FP64 CSR, warp per row)"),
+                         "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
                          "traffic": traffic, "peak_source": peak_kind,
@@ -338,11 +372,42 @@ def run_ours(args):
                              if cpu else None),
         }
     s.close()
+    if line is not None and mixed:
+        line["error_vs_fp64"] = mixed_vs_fp64(vm, cfg, case, scenes, dev, steps=10)
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     if line:
         print(json.dumps(line), flush=True)
+
+
+def mixed_vs_fp64(vm, cfg, case, scenes, dev, steps):
+    """Max relative differences between the mixed-precision run and the FP64
+    run of the same case after the same number of steps (not timed)."""
+    import numpy as np
+    out = {}
+    for prec in (1, 0):
+        c = dict(cfg)
+        c["precision"] = prec
+        s = vm.Solver(c, case, device=dev)
+        if scenes is not None:
+            s.set_scenes(*scenes)
+        s.init()
+        p1 = None
+        for k in range(steps):
+            s.step()
+            if k == 0:
+                p1 = s.get("p")
+        out[prec] = {"p_step1": p1, **{f: s.get(f) for f in ("x", "y", "z", "u", "v", "w", "p")}}
+        s.close()
+
+    def rel(a, b):
+        return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+    res = {"steps": steps, "norm": "max|mixed - fp64| / max|fp64|",
+           "p_after_1_step": rel(out[1]["p_step1"], out[0]["p_step1"])}
+    for f in ("p", "x", "y", "z", "u", "v", "w"):
+        res[f] = rel(out[1][f], out[0][f])
+    return res
 
 
 def main():
@@ -353,7 +418,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--graph", type=int, default=1, choices=[0, 1],
                     help="1: each step is one CUDA graph launch (CG loop as a while node)")
-    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 3, 4],
+    ap.add_argument("--precision", type=int, default=None, choices=[0, 1],
+                    help="PPE precision (default: mixed for configs 2 and 4, FP64 otherwise)")
+    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2, 3, 4],
                     help="benchmark configuration (1: the headline 3D dam break)")
     ap.add_argument("--scale", type=int, default=0,
                     help="profiling only: smaller 3D dam (10s x 20s x 10s fluid)")

@@ -34,3 +34,22 @@ def rel_err(a, b):
 
 def lists_equal(g_off, g_nbr, o_off, o_nbr):
     return np.array_equal(g_off, o_off) and np.array_equal(g_nbr, o_nbr)
+
+
+def oracle_relres(g, cfg):
+    """||b - A x|| / ||b|| of the GPU's pressure in the oracle's own FP64
+    system, assembled by the oracle from the GPU's lists and positions."""
+    import ctypes as C
+    lib = pyoracle.oracle_lib()
+    P = pyoracle.params_from(cfg)
+    n = g.n
+    goff, gnbr = g.lists(1)
+    xs, ys, zs = g.get("xs"), g.get("ys"), g.get("zs")
+    bcon, src, p = g.get("bcon"), g.get("source"), g.get("pnew")
+    diag, val = np.zeros(n), np.zeros(max(len(gnbr), 1))
+    ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    lib.mo_matrix(C.byref(P), cfg["re_l"], lib.mo_lambda(cfg["ktype"], cfg["re_l"]),
+                  g.scalar("n0_l"), n, ip(goff), ip(gnbr), dp(xs), dp(ys), dp(zs), ip(bcon),
+                  dp(diag), dp(val))
+    return lib.mo_relres(n, ip(goff), ip(gnbr), ip(bcon), dp(diag), dp(val), dp(src), dp(p))

@@ -132,7 +132,7 @@ int validate(const mps_config& f, std::string& why)
     }
     if (f.solver != 1 && f.solver != 2) { why = "solver must be 1 (Jacobi-PCG) or 2 (CG)"; return MPS_ERR_ARG; }
     if (f.warm_start < 0 || f.warm_start > 2) { why = "warm_start must be 0, 1 or 2"; return MPS_ERR_ARG; }
-    if (f.precision != 0) { why = "precision 1 (mixed) is not available in this build"; return MPS_ERR_ARG; }
+    if (f.precision != 0 && f.precision != 1) { why = "precision must be 0 (FP64) or 1 (mixed)"; return MPS_ERR_ARG; }
     return MPS_OK;
 }
 
@@ -241,6 +241,11 @@ int allocate(mps_ctx* c)
     TRY(dalloc(c, &c->nbr_s, (size_t)c->cap_s * P));
     TRY(dalloc(c, &c->mcol, (size_t)c->cap_l * P));
     TRY(dalloc(c, &c->mval, (size_t)c->cap_l * P));
+    if (c->cfg.precision == 1) {
+        TRY(dalloc(c, &c->mval32, (size_t)c->cap_l * P));
+        float** ffields[] = {&c->ir_d, &c->ir_r, &c->ir_z, &c->ir_p, &c->ir_s};
+        for (auto f : ffields) TRY(dalloc(c, f, P));
+    }
     int sms = 0;
     VMPS_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
     // CG partials: 5 arrays of one value per block, at most 8 blocks per SM
@@ -622,7 +627,8 @@ int mps_step(mps_ctx* c)
     c->steps++;
     int e = collect_errors(c);
     TRY(vmps_ppe_finish(c));
-    if (graph && c->cfg.method != 3) vmps_count_launch(c->cg_iters * c->cg_loop_kernels);
+    if (graph && c->cfg.method != 3)
+        vmps_count_launch((c->cg_iters + c->cg_outer) * c->cg_loop_kernels);
     if (c->profile) {
         for (int k = 0; k < 4; k++) {
             float ms = 0;
@@ -798,6 +804,7 @@ int mps_get_scalar(mps_ctx* c, const char* name, double* out)
     else if (s == "lambda_l") *out = c->lambda_l;
     else if (s == "cg_iters") *out = c->cg_iters;
     else if (s == "cg_relres") *out = c->cg_relres;
+    else if (s == "cg_outer") *out = c->cg_outer;
     else if (s == "n") *out = c->n;
     else if (s == "steps") *out = (double)c->steps;
     else if (s == "cap_s") *out = c->cap_s;

@@ -151,6 +151,11 @@ struct mps_ctx {
     double* mval = nullptr;
     double *pres_x = nullptr, *pres_y = nullptr, *pres_z = nullptr;  // prediction pressure sums
     double *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_s = nullptr;
+    // mixed precision (precision 1): FP32 copy of the matrix values and the
+    // FP32 inner-CG vectors (correction d, residual, z, direction, A p)
+    float* mval32 = nullptr;
+    float *ir_d = nullptr, *ir_r = nullptr, *ir_z = nullptr, *ir_p = nullptr, *ir_s = nullptr;
+    int cg_outer = 0;
     double* cg_part = nullptr;   // block partial sums
     size_t cg_part_cap = 0;      // doubles in cg_part
     double* cg_scal = nullptr;   // device scalars (rz, bb, rr, ...)
@@ -301,6 +306,11 @@ struct Grp {
     }
     // sum over the group, result in every lane (fixed butterfly order)
     __device__ __forceinline__ double sum(double v) const
+    {
+        for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+        return v;
+    }
+    __device__ __forceinline__ float sumf(float v) const
     {
         for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
         return v;

@@ -19,7 +19,13 @@ using namespace vmps;
 
 namespace {
 
-enum { S_BB = 0, S_RZ, S_RR, S_ZERO, S_NEWRZ, S_NEWRR, S_DONE, S_WORST, S_COUNT };
+enum {
+    S_BB = 0, S_RZ, S_RR, S_ZERO, S_NEWRZ, S_NEWRR, S_DONE, S_WORST,
+    // mixed precision: inner r.r, its value at the sweep's start, the sweep's
+    // target reduction (squared), the staged inner stop, staged inner r.r
+    S_RIN, S_RIN0, S_ETA2, S_INDONE, S_NEWRIN, S_COUNT
+};
+static_assert(S_COUNT <= 16, "cg_scal and red_host hold 16 doubles");
 constexpr int kRedThreads = 256;
 
 __device__ __forceinline__ double block_sum(double v, double* sh)
@@ -66,8 +72,8 @@ __global__ void __launch_bounds__(256, 5) k_assemble(int n, int cap, Asm A, cons
                            int warm, double* __restrict__ pnew, double* __restrict__ pold,
                            const int* __restrict__ moff,
                            int* __restrict__ mcol, double* __restrict__ mval,
-                           int* __restrict__ mlen, double* __restrict__ diag,
-                           double* __restrict__ source)
+                           float* __restrict__ mval32, int* __restrict__ mlen,
+                           double* __restrict__ diag, double* __restrict__ source)
 {
     Grp<32> q;
     int i = (int)q.gid;
@@ -113,6 +119,7 @@ __global__ void __launch_bounds__(256, 5) k_assemble(int n, int cap, Asm A, cons
             int pos = cnt + __popc(m & ((1u << q.lane) - 1u));
             crow[pos] = j;
             vrow[pos] = -v;
+            if (mval32) mval32[moff[i] + pos] = (float)(-v);
         }
         cnt += __popc(m);
     }
@@ -203,8 +210,9 @@ struct CG {
 // butterfly sum in a fixed order; every lane returns the row's value.  (This
 // plain form runs at 32 registers; restructured or deeper-unrolled variants
 // measured 15-70% slower on B200.)
+template <typename V>
 __device__ __forceinline__ double spmv_row_warp(const CG& A, const Grp<32>& q,
-                                                const double* __restrict__ v, int i)
+                                                const V* __restrict__ v, int i)
 {
     const int L = A.mlen[i];
     const int* __restrict__ c = A.mcol + A.moff[i];
@@ -214,12 +222,46 @@ __device__ __forceinline__ double spmv_row_warp(const CG& A, const Grp<32>& q,
     for (; k + 32 < L; k += 64) {
         int c0 = __ldg(c + k), c1 = __ldg(c + k + 32);
         double a0 = __ldg(a + k), a1 = __ldg(a + k + 32);
+        acc0 += a0 * (double)v[c0];
+        acc1 += a1 * (double)v[c1];
+    }
+    if (k < L) acc0 += __ldg(a + k) * (double)v[__ldg(c + k)];
+    double acc = q.sum(acc0 + acc1);
+    return A.diag[i] * (double)v[i] + acc;
+}
+
+// (A32 v)_i for the inner solve of the mixed-precision path: FP32 values,
+// FP32 products and accumulation, same warp-per-row layout.  FP32 halves
+// the bytes of each load, so each lane keeps four column/value pairs in
+// flight (instead of two) to hold the same bytes in flight per warp.
+__device__ __forceinline__ float spmv_row_warp32(const CG& A, const float* __restrict__ val,
+                                                 const Grp<32>& q, const float* __restrict__ v,
+                                                 int i)
+{
+    const int L = A.mlen[i];
+    const int* __restrict__ c = A.mcol + A.moff[i];
+    const float* __restrict__ a = val + A.moff[i];
+    float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc3 = 0.f;
+    int k = q.lane;
+    for (; k + 96 < L; k += 128) {
+        int c0 = __ldg(c + k), c1 = __ldg(c + k + 32), c2 = __ldg(c + k + 64),
+            c3 = __ldg(c + k + 96);
+        float a0 = __ldg(a + k), a1 = __ldg(a + k + 32), a2 = __ldg(a + k + 64),
+              a3 = __ldg(a + k + 96);
+        acc0 += a0 * v[c0];
+        acc1 += a1 * v[c1];
+        acc2 += a2 * v[c2];
+        acc3 += a3 * v[c3];
+    }
+    for (; k + 32 < L; k += 64) {
+        int c0 = __ldg(c + k), c1 = __ldg(c + k + 32);
+        float a0 = __ldg(a + k), a1 = __ldg(a + k + 32);
         acc0 += a0 * v[c0];
         acc1 += a1 * v[c1];
     }
-    if (k < L) acc0 += __ldg(a + k) * v[__ldg(c + k)];
-    double acc = q.sum(acc0 + acc1);
-    return A.diag[i] * v[i] + acc;
+    if (k < L) acc2 += __ldg(a + k) * v[__ldg(c + k)];
+    float acc = q.sumf((acc0 + acc1) + (acc2 + acc3));
+    return (float)A.diag[i] * v[i] + acc;
 }
 
 // r = b - A x, z = M^-1 r, p = z; partials of b.b, r.z, r.r
@@ -375,6 +417,7 @@ __global__ void k_scene_sums(int mode, const int* __restrict__ first, const int*
 {
     __shared__ double sh[33];
     if (flag && flag[0]) return;
+    if (mode == 2 && flag[2] != 1) return;  // mixed precision: refinements only
     int k = blockIdx.x;
     double acc = 0.0;
     for (int i = first[k] + threadIdx.x; i < last[k]; i += blockDim.x)
@@ -439,6 +482,250 @@ __global__ void k_clamp(int n, double pmin, double pmax, const double* __restric
     pnew[i] = v;
 }
 
+
+// ---------------------------------------------------------------------------
+// Mixed precision (precision 1): iterative refinement.  The outer loop keeps
+// x and r = b - A x in FP64 (r is updated as r -= A64 d with the FP64 matrix,
+// so its accuracy is FP64's); each sweep solves A32 d = r approximately by
+// Jacobi-PCG in FP32 (FP32 matrix copy, FP32 vectors, FP32 SpMV sums) with
+// FP64 dot products, until the inner residual has fallen by the sweep's
+// target factor.  The stop test is the FP64 one: ||r||/||b|| <= cg_tol.
+//
+// Both loops are one device state machine so that the graph's single while
+// node (or the eager host loop) drives them: flag[2] = 0 runs an inner CG
+// iteration, flag[2] = 1 runs a refinement; flag[1] counts inner iterations
+// and flag[3] refinements.
+struct IR {
+    const float* __restrict__ val;  // FP32 copy of the CSR values
+    float* __restrict__ d;          // correction of this sweep
+    float* __restrict__ r;          // inner residual
+    float* __restrict__ z;
+    float* __restrict__ p;
+    float* __restrict__ s;
+};
+
+constexpr int kMaxSweeps = 40;  // refinement sweeps per solve (bound)
+
+__host__ __device__ __forceinline__ double sweep_target(double tol2, double bb, double rr)
+{
+    // reduce the inner residual by what the FP64 test still needs (with a
+    // factor 2 margin), at least 10x and at most to 1e-5 (FP32's floor)
+    double e = rr > 0 ? 0.25 * tol2 * bb / rr : 1e-10;
+    return fmin(1e-2, fmax(1e-10, e));
+}
+
+// r64 = b - A64 x; r32 = r64; z = M^-1 r32; p = z; d = 0; partials b.b,
+// r32.z, r64.r64, r32.r32
+__global__ void k_ir_start(CG A, IR I, const double* __restrict__ b, const double* __restrict__ x,
+                           double* __restrict__ r64, double* __restrict__ part)
+{
+    __shared__ double sh[33];
+    Grp<32> q;
+    const long nwarps = (long)gridDim.x * blockDim.x / 32;
+    double bb = 0, rz = 0, rr = 0, rin = 0;
+    for (long w = q.gid; w < A.n; w += nwarps) {
+        int i = (int)w;
+        double ri = 0;
+        float r32 = 0.f, z32 = 0.f;
+        if (A.bcon[i] == 0) {
+            double bi = b[i];
+            ri = bi - spmv_row_warp(A, q, x, i);
+            r32 = (float)ri;
+            z32 = A.precond ? r32 / (float)A.diag[i] : r32;
+            if (q.lane == 0) {
+                bb += bi * bi;
+                rr += ri * ri;
+                rz += (double)r32 * (double)z32;
+                rin += (double)r32 * (double)r32;
+            }
+        }
+        if (q.lane == 0) {
+            r64[i] = ri;
+            I.r[i] = r32;
+            I.z[i] = z32;
+            I.p[i] = z32;
+            I.d[i] = 0.f;
+            I.s[i] = 0.f;
+        }
+    }
+    bb = block_sum(bb, sh);
+    rz = block_sum(rz, sh);
+    rr = block_sum(rr, sh);
+    rin = block_sum(rin, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = bb;
+        part[A.nparts + blockIdx.x] = rz;
+        part[2 * A.nparts + blockIdx.x] = rr;
+        part[3 * A.nparts + blockIdx.x] = rin;
+    }
+}
+
+__global__ void k_ir_start_scalars(int nparts, const double* __restrict__ part, double tol2,
+                                   double* scal, int* flag, int use_cond,
+                                   cudaGraphConditionalHandle cond)
+{
+    __shared__ double sh[33];
+    double bb = reduce_parts(part, nparts, sh);
+    double rz = reduce_parts(part + nparts, nparts, sh);
+    double rr = reduce_parts(part + 2 * nparts, nparts, sh);
+    double rin = reduce_parts(part + 3 * nparts, nparts, sh);
+    if (threadIdx.x == 0) {
+        scal[S_BB] = bb;
+        scal[S_RZ] = rz;
+        scal[S_RR] = rr;
+        scal[S_RIN] = rin;
+        scal[S_RIN0] = rin;
+        scal[S_ETA2] = sweep_target(tol2, bb, rr);
+        scal[S_ZERO] = (bb == 0.0) ? 1.0 : 0.0;
+        flag[0] = (bb == 0.0 || rr <= tol2 * bb) ? 1 : 0;
+        flag[1] = 0;
+        flag[2] = 0;
+        flag[3] = 0;
+        if (use_cond) cudaGraphSetConditional(cond, flag[0] ? 0u : 1u);
+    }
+}
+
+// inner: s = A32 p, partial p.s.  refinement: r64 -= A64 d, x += d, partial
+// r64.r64 (each row writes only its own x and r; d is read-only here)
+__global__ void k_ir_spmv(CG A, IR I, double* __restrict__ r64, double* __restrict__ x,
+                          double* __restrict__ part, const int* __restrict__ flag)
+{
+    __shared__ double sh[33];
+    if (flag[0]) return;
+    const int phase = flag[2];
+    Grp<32> q;
+    const long nwarps = (long)gridDim.x * blockDim.x / 32;
+    double acc = 0;
+    for (long w = q.gid; w < A.n; w += nwarps) {
+        int i = (int)w;
+        if (A.bcon[i] != 0) {
+            if (phase == 0 && q.lane == 0) I.s[i] = 0.f;
+            continue;
+        }
+        if (phase == 0) {
+            float si = spmv_row_warp32(A, I.val, q, I.p, i);
+            if (q.lane == 0) {
+                I.s[i] = si;
+                acc += (double)I.p[i] * (double)si;
+            }
+        } else {
+            double t = spmv_row_warp(A, q, I.d, i);
+            if (q.lane == 0) {
+                double ri = r64[i] - t;
+                r64[i] = ri;
+                x[i] = x[i] + (double)I.d[i];
+                acc += ri * ri;
+            }
+        }
+    }
+    acc = block_sum(acc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+// inner: alpha = rz / p.s; d += alpha p; r -= alpha s.  refinement: r32 =
+// r64, d = 0.  Then z = M^-1 r32 and partials r32.z, r32.r32 (FP64 sums).
+__global__ void k_ir_update(CG A, IR I, const double* __restrict__ r64,
+                            const double* __restrict__ part_ps, double* __restrict__ part,
+                            const double* __restrict__ scal, const int* __restrict__ flag)
+{
+    __shared__ double sh[33];
+    if (flag[0]) return;
+    const int phase = flag[2];
+    float alpha = 0.f;
+    if (phase == 0) {
+        double ps = reduce_parts(part_ps, A.nparts, sh);
+        alpha = (float)(scal[S_RZ] / ps);
+    }
+    double rz = 0, rin = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+        if (A.bcon[i] != 0) continue;
+        float ri;
+        if (phase == 0) {
+            I.d[i] = I.d[i] + alpha * I.p[i];
+            ri = I.r[i] - alpha * I.s[i];
+        } else {
+            I.d[i] = 0.f;
+            ri = (float)r64[i];
+        }
+        float zi = A.precond ? ri / (float)A.diag[i] : ri;
+        I.r[i] = ri;
+        I.z[i] = zi;
+        rz += (double)ri * (double)zi;
+        rin += (double)ri * (double)ri;
+    }
+    rz = block_sum(rz, sh);
+    rin = block_sum(rin, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = rz;
+        part[A.nparts + blockIdx.x] = rin;
+    }
+}
+
+// inner: beta = rz'/rz, p = z + beta p unless the sweep ends.  refinement:
+// the FP64 stop test (per scene when batched); p = z starts the next sweep.
+__global__ void k_ir_direction(CG A, IR I, const double* __restrict__ part,
+                               const double* __restrict__ part_rr, double* scal,
+                               const int* __restrict__ flag, double tol2, int maxit, int nscenes,
+                               const int* __restrict__ sok)
+{
+    __shared__ double sh[33];
+    if (flag[0]) return;
+    const int phase = flag[2];
+    double rz = reduce_parts(part, A.nparts, sh);
+    double rin = reduce_parts(part + A.nparts, A.nparts, sh);
+    bool restart = false, indone = false, done = false;
+    double rr = 0, beta = 0;
+    if (phase == 0) {
+        beta = rz / scal[S_RZ];
+        int it = flag[1] + 1;
+        indone = rin <= scal[S_ETA2] * scal[S_RIN0] || it >= maxit || !(rin == rin);
+    } else {
+        rr = reduce_parts(part_rr, A.nparts, sh);
+        bool conv = rr <= tol2 * scal[S_BB];
+        if (nscenes > 1) {
+            conv = true;
+            for (int k = 0; k < nscenes; k++) conv = conv && (sok[k] != 0);
+        }
+        done = conv || flag[1] >= maxit || flag[3] + 1 >= kMaxSweeps || !(rr == rr);
+        restart = !done;
+    }
+    if ((phase == 0 && !indone) || restart) {
+        const float b32 = (float)beta;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x)
+            if (A.bcon[i] == 0) I.p[i] = restart ? I.z[i] : I.z[i] + b32 * I.p[i];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        scal[S_NEWRZ] = rz;
+        scal[S_NEWRIN] = rin;
+        scal[S_INDONE] = indone ? 1.0 : 0.0;
+        if (phase == 1) {
+            scal[S_NEWRR] = rr;
+            scal[S_DONE] = done ? 1.0 : 0.0;
+        }
+    }
+}
+
+__global__ void k_ir_commit(double* scal, int* flag, double tol2, int use_cond,
+                            cudaGraphConditionalHandle cond)
+{
+    if (!flag[0]) {
+        scal[S_RZ] = scal[S_NEWRZ];
+        scal[S_RIN] = scal[S_NEWRIN];
+        if (flag[2] == 0) {
+            flag[1] += 1;
+            if (scal[S_INDONE] != 0.0) flag[2] = 1;
+        } else {
+            scal[S_RR] = scal[S_NEWRR];
+            scal[S_RIN0] = scal[S_NEWRIN];
+            scal[S_ETA2] = sweep_target(tol2, scal[S_BB], scal[S_RR]);
+            flag[3] += 1;
+            flag[2] = 0;
+            if (scal[S_DONE] != 0.0) flag[0] = 1;
+        }
+    }
+    if (use_cond) cudaGraphSetConditional(cond, flag[0] ? 0u : 1u);
+}
+
 }  // namespace
 
 int vmps_ppe(mps_ctx* c)
@@ -469,11 +756,11 @@ int vmps_ppe(mps_ctx* c)
     if (f.dim == 3)
         k_assemble<3><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
                                                   nsrc, f.warm_start, c->pnew, c->pold, c->moff, c->mcol,
-                                                  c->mval, c->mlen, c->diag, c->source);
+                                                  c->mval, c->mval32, c->mlen, c->diag, c->source);
     else
         k_assemble<2><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
                                                   nsrc, f.warm_start, c->pnew, c->pold, c->moff, c->mcol,
-                                                  c->mval, c->mlen, c->diag, c->source);
+                                                  c->mval, c->mval32, c->mlen, c->diag, c->source);
     vmps_count_launch(1);
     if (f.srcopt) {
         // slot of particle id k: inv_id[k] (the sort's inv buffer is free here)
@@ -510,10 +797,18 @@ int vmps_ppe(mps_ctx* c)
     const bool graph = cap == cudaStreamCaptureStatusActive;
     cudaGraphConditionalHandle cond = 0;
     if (graph) VMPS_CUDA(c, cudaGraphConditionalHandleCreate(&cond, cgraph, 1, cudaGraphCondAssignDefault));
-    k_cg_start<<<nblk, kRedThreads, 0, st>>>(G, c->source, c->pnew, c->cg_r, c->cg_z, c->cg_p,
-                                             c->cg_part);
-    k_cg_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal, c->cg_flag,
-                                                  graph ? 1 : 0, cond);
+    const bool mixed = f.precision == 1;
+    IR I{c->mval32, c->ir_d, c->ir_r, c->ir_z, c->ir_p, c->ir_s};
+    if (mixed) {
+        k_ir_start<<<nblk, kRedThreads, 0, st>>>(G, I, c->source, c->pnew, c->cg_r, c->cg_part);
+        k_ir_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal,
+                                                      c->cg_flag, graph ? 1 : 0, cond);
+    } else {
+        k_cg_start<<<nblk, kRedThreads, 0, st>>>(G, c->source, c->pnew, c->cg_r, c->cg_z,
+                                                 c->cg_p, c->cg_part);
+        k_cg_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal,
+                                                      c->cg_flag, graph ? 1 : 0, cond);
+    }
     vmps_count_launch(2);
     if (batched) {
         k_scene_sums<<<c->nscenes, kRedThreads, 0, st>>>(0, c->sfirst, c->slast, c->scene, c->bcon,
@@ -530,6 +825,23 @@ int vmps_ppe(mps_ctx* c)
                 c->ev_spmv.push_back(e);
             }
             VMPS_CUDA(c, cudaEventRecord(c->ev_spmv[2 * k], s));
+        }
+        if (mixed) {
+            k_ir_spmv<<<nblk, kRedThreads, 0, s>>>(G, I, c->cg_r, c->pnew, c->cg_part + 4 * nblk,
+                                                   c->cg_flag);
+            if (c->profile && !graph) VMPS_CUDA(c, cudaEventRecord(c->ev_spmv[2 * k + 1], s));
+            if (batched)
+                k_scene_sums<<<c->nscenes, kRedThreads, 0, s>>>(2, c->sfirst, c->slast, c->scene,
+                                                                c->bcon, c->cg_r, tol2, c->sbb,
+                                                                c->srr, c->sok, c->cg_flag);
+            k_ir_update<<<nblk, kRedThreads, 0, s>>>(G, I, c->cg_r, c->cg_part + 4 * nblk,
+                                                     c->cg_part, c->cg_scal, c->cg_flag);
+            k_ir_direction<<<nblk, kRedThreads, 0, s>>>(G, I, c->cg_part, c->cg_part + 4 * nblk,
+                                                        c->cg_scal, c->cg_flag, tol2, f.cg_max,
+                                                        c->nscenes, c->sok);
+            k_ir_commit<<<1, 1, 0, s>>>(c->cg_scal, c->cg_flag, tol2, graph ? 1 : 0, cond);
+            VMPS_CUDA(c, cudaGetLastError());
+            return MPS_OK;
         }
         k_cg_spmv<<<nblk, kRedThreads, 0, s>>>(G, c->cg_p, c->cg_s, c->cg_part + 4 * nblk,
                                                c->cg_flag);
@@ -574,13 +886,15 @@ int vmps_ppe(mps_ctx* c)
         if (r != MPS_OK) return r;
     } else {
         const int check = 4;
-        for (int it = 0; it < f.cg_max; it++) {
+        // the mixed path's body alternates inner iterations and refinements
+        const int bound = mixed ? f.cg_max + kMaxSweeps : f.cg_max;
+        for (int it = 0; it < bound; it++) {
             int r = iteration(st, it);
             if (r != MPS_OK) return r;
             vmps_count_launch(c->cg_loop_kernels);
             c->cg_nspmv++;
-            if ((it + 1) % check == 0 || it + 1 == f.cg_max) {
-                VMPS_CUDA(c, cudaMemcpyAsync(c->cg_flag_host, c->cg_flag, 2 * sizeof(int),
+            if ((it + 1) % check == 0 || it + 1 == bound) {
+                VMPS_CUDA(c, cudaMemcpyAsync(c->cg_flag_host, c->cg_flag, 4 * sizeof(int),
                                              cudaMemcpyDeviceToHost, st));
                 VMPS_CUDA(c, cudaStreamSynchronize(st));
                 if (c->cg_flag_host[0]) break;
@@ -594,7 +908,7 @@ int vmps_ppe(mps_ctx* c)
     k_clamp<<<grid_blocks(n), kBlock, 0, st>>>(n, f.pmin, f.pmax, c->cg_scal, c->pnew,
                                                batched ? c->scene : nullptr, c->spmax, c->sbb);
     vmps_count_launch(1);
-    VMPS_CUDA(c, cudaMemcpyAsync(c->cg_flag_host, c->cg_flag, 2 * sizeof(int),
+    VMPS_CUDA(c, cudaMemcpyAsync(c->cg_flag_host, c->cg_flag, 4 * sizeof(int),
                                  cudaMemcpyDeviceToHost, st));
     VMPS_CUDA(c, cudaMemcpyAsync(c->red_host, c->cg_scal, S_COUNT * sizeof(double),
                                  cudaMemcpyDeviceToHost, st));
@@ -610,9 +924,11 @@ int vmps_ppe_finish(mps_ctx* c)
     c->ppe_pending = false;
     const mps_config& f = c->cfg;
     c->cg_iters = c->cg_flag_host[1];
+    c->cg_outer = f.precision == 1 ? c->cg_flag_host[3] : 0;
     if (c->profile) {
         // launches after convergence exit at once: count the working ones
-        for (int k = 0; k < c->cg_nspmv && k < c->cg_iters; k++) {
+        const int working = c->cg_iters + c->cg_outer;
+        for (int k = 0; k < c->cg_nspmv && k < working; k++) {
             float ms = 0;
             VMPS_CUDA(c, cudaEventElapsedTime(&ms, c->ev_spmv[2 * k], c->ev_spmv[2 * k + 1]));
             c->spmv_ms += ms;
