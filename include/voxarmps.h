@@ -160,6 +160,33 @@ int mps_set_profile(mps_ctx* ctx, int on);
  * one graph launch and one host synchronisation per step.  Results are
  * identical to eager mode.  Off while profiling (mps_set_profile). */
 int mps_set_graph(mps_ctx* ctx, int on);
+
+/* ---- learned CG initial guess (no reference counterpart) ---------------- *
+ * A message-passing network on the PND-radius neighbour graph (hidden width
+ * 64, `layers` residual layers, BF16 weights/activations, FP32 sums) maps
+ * per-particle inputs (PND deviation, previous pressure, particle kind) to
+ * the pressure increment of the coming solve.  While a network exists every
+ * PPE captures its inputs; mps_gnn_train then fits the network to the
+ * pressure that PPE solved for.  With mps_gnn_use(ctx, 1) the prediction is
+ * CG's starting point; CG still runs to cg_tol, so only the iteration count
+ * changes.  Weights start from SplitMix64(seed) with a zero output layer
+ * (the untrained guess is the previous pressure). */
+int mps_gnn_create(mps_ctx* ctx, int layers, unsigned long long seed);
+int mps_gnn_use(mps_ctx* ctx, int on);
+/* `iters` Adam steps (learning rate lr) on the last PPE.  objective 0: mean
+ * squared error of the scaled pressure increment against the solved one;
+ * objective 1: relative squared residual |b - A x0|^2/|b|^2 that the guess
+ * x0 leaves in that PPE's system.  grad_only != 0 only computes the
+ * gradient.  *loss = the objective before the last update. */
+int mps_gnn_train(mps_ctx* ctx, int iters, float lr, int objective, int grad_only, float* loss);
+/* copy the FP32 parameters out (get) and/or in (set, resets Adam); *count = P */
+int mps_gnn_params(mps_ctx* ctx, float* get, const float* set, int* count);
+/* inputs of the current state / forward pass on the captured inputs */
+int mps_gnn_features(mps_ctx* ctx);
+int mps_gnn_forward(mps_ctx* ctx);
+/* network data in slot (cell) order: "feat", "target", "y", "grad", "pref",
+ * "count", "nbr", "len", "bcon", "ptype", "cap" */
+int mps_gnn_download(mps_ctx* ctx, const char* what, void* out, long* count);
 /* Scalars: n0_s n0_l lambda_l cg_iters cg_relres n nnz_s nnz_l nnz_a steps
  * cap_s cap_l len_max_s len_max_l launches pmax and the profile timings. */
 int mps_get_scalar(mps_ctx* ctx, const char* name, double* out);

@@ -45,6 +45,8 @@ EXPORTS = [
     "mps_download_lists", "mps_get_scalar", "mps_get_error", "mps_last_message",
     "mps_write_vtu", "mps_stream", "mps_set_state", "mps_get_state", "mps_set_profile",
     "mps_cell_order_noalloc", "mps_set_scenes", "mps_set_graph",
+    "mps_gnn_create", "mps_gnn_use", "mps_gnn_train", "mps_gnn_params", "mps_gnn_features",
+    "mps_gnn_forward", "mps_gnn_download",
 ]
 
 _LIB = None
@@ -90,6 +92,14 @@ def load_library(path: str = LIB_PATH):
     lib.mps_get_state.argtypes = [P, P, P, P, P, P, P, P]
     lib.mps_set_profile.argtypes = [P, C.c_int]
     lib.mps_set_graph.argtypes = [P, C.c_int]
+    FP = C.POINTER(C.c_float)
+    lib.mps_gnn_create.argtypes = [P, C.c_int, C.c_ulonglong]
+    lib.mps_gnn_use.argtypes = [P, C.c_int]
+    lib.mps_gnn_train.argtypes = [P, C.c_int, C.c_float, C.c_int, C.c_int, FP]
+    lib.mps_gnn_params.argtypes = [P, FP, FP, C.POINTER(C.c_int)]
+    lib.mps_gnn_features.argtypes = [P]
+    lib.mps_gnn_forward.argtypes = [P]
+    lib.mps_gnn_download.argtypes = [P, C.c_char_p, P, C.POINTER(C.c_long)]
     lib.mps_set_scenes.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
                                    C.POINTER(C.c_double)]
     lib.mps_cell_order_noalloc.argtypes = [C.POINTER(MpsConfig), C.c_double, C.c_int, P, P, P,
@@ -240,6 +250,51 @@ class Solver:
 
     def set_profile(self, on: bool = True):
         return self._chk(self.lib.mps_set_profile(self.h, int(on)), "profile")
+
+    # ---- learned CG initial guess -------------------------------------
+    def gnn_create(self, layers: int = 4, seed: int = 0):
+        return self._chk(self.lib.mps_gnn_create(self.h, layers, seed), "gnn_create")
+
+    def gnn_use(self, on: bool = True):
+        return self._chk(self.lib.mps_gnn_use(self.h, int(on)), "gnn_use")
+
+    def gnn_train(self, iters: int = 1, lr: float = 1e-3, grad_only: bool = False,
+                  objective: str = "residual") -> float:
+        """Adam steps on the last PPE; objective "residual" (|b - A x0|^2/|b|^2)
+        or "increment" (squared error of the scaled pressure increment)."""
+        obj = {"increment": 0, "residual": 1}[objective]
+        loss = C.c_float()
+        self._chk(self.lib.mps_gnn_train(self.h, iters, lr, obj, int(grad_only), C.byref(loss)),
+                  "gnn_train")
+        return loss.value
+
+    def gnn_params(self, set_to=None) -> np.ndarray:
+        cnt = C.c_int()
+        self._chk(self.lib.mps_gnn_params(self.h, None, None, C.byref(cnt)), "gnn_params")
+        out = np.zeros(cnt.value, np.float32)
+        src = None
+        if set_to is not None:
+            src = np.ascontiguousarray(set_to, np.float32)
+            assert src.size == cnt.value
+            src = src.ctypes.data_as(C.POINTER(C.c_float))
+        self._chk(self.lib.mps_gnn_params(self.h, out.ctypes.data_as(C.POINTER(C.c_float)), src,
+                                          None), "gnn_params")
+        return out
+
+    def gnn_features(self):
+        return self._chk(self.lib.mps_gnn_features(self.h), "gnn_features")
+
+    def gnn_forward(self):
+        return self._chk(self.lib.mps_gnn_forward(self.h), "gnn_forward")
+
+    def gnn_get(self, what: str) -> np.ndarray:
+        cnt = C.c_long()
+        self._chk(self.lib.mps_gnn_download(self.h, what.encode(), None, C.byref(cnt)), what)
+        dt = np.int32 if what in ("nbr", "len", "cap", "bcon", "ptype") else np.float32
+        out = np.zeros(max(cnt.value, 1), dt)
+        self._chk(self.lib.mps_gnn_download(self.h, what.encode(), out.ctypes.data_as(C.c_void_p),
+                                            None), what)
+        return out[:cnt.value]
 
     def set_graph(self, on: bool = True):
         """Replay each step as one CUDA graph (CG loop as a while node)."""

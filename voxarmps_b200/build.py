@@ -12,7 +12,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libvoxarmps_b200.so")
-SOURCES = ["mps_context.cu", "mps_neighbors.cu", "mps_stages.cu", "mps_ppe.cu", "mps_noalloc.cu"]
+SOURCES = ["mps_context.cu", "mps_neighbors.cu", "mps_stages.cu", "mps_ppe.cu", "mps_noalloc.cu",
+           "mps_gnn.cu"]
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC",

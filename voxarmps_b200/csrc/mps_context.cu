@@ -291,6 +291,8 @@ double* field_d(mps_ctx* c, const std::string& f)
 
 }  // namespace
 
+void vmps_drop_graphs(mps_ctx* c) { drop_graphs(c); }
+
 std::vector<void*>& vmps_reorder_alts(mps_ctx* ctx) { return ctx->alts; }
 
 // ------------------------------------------------------------------ C-ABI
@@ -325,6 +327,7 @@ int mps_destroy(mps_ctx* c)
 {
     if (!c) return MPS_OK;
     free_all(c);
+    vmps_gnn_free(c);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : c->ev_spmv) cudaEventDestroy(e);
@@ -341,6 +344,7 @@ int mps_upload(mps_ctx* c, int n, const double* x, const double* y, const double
     if (!c || n <= 0 || !x || !y || !ptype || (c->cfg.dim == 3 && !z)) return MPS_ERR_ARG;
     VMPS_CUDA(c, cudaSetDevice(c->device));
     free_all(c);
+    vmps_gnn_reset(c);
     mps_config& f = c->cfg;
     c->n = n;
     c->nscenes = 1;
@@ -589,6 +593,7 @@ static int graph_step(mps_ctx* c)
 {
     const int par = (int)(c->swaps & 1);
     if (!c->stream2) VMPS_CUDA(c, cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
+    TRY(vmps_gnn_prepare(c));  // no allocation inside the capture
     if (!c->gexec[par]) {
         const long long l0 = g_launches.load();
         VMPS_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
@@ -804,6 +809,7 @@ int mps_get_scalar(mps_ctx* c, const char* name, double* out)
     else if (s == "lambda_l") *out = c->lambda_l;
     else if (s == "cg_iters") *out = c->cg_iters;
     else if (s == "cg_relres") *out = c->cg_relres;
+    else if (s == "cg_r0") *out = c->cg_r0;
     else if (s == "cg_outer") *out = c->cg_outer;
     else if (s == "n") *out = c->n;
     else if (s == "steps") *out = (double)c->steps;

@@ -81,6 +81,8 @@ inline WK make_wk(int ktype, double re)
 
 }  // namespace vmps
 
+struct vmps_gnn;  // learned CG initial guess (mps_gnn.cu)
+
 struct mps_ctx {
     mps_config cfg;
     int device = 0;
@@ -93,6 +95,7 @@ struct mps_ctx {
     double cut_l = 0, cut_s = 0;  // squared-distance thresholds
     int cap_l = 0, cap_s = 0;
     double n0_s = 0, n0_l = 0, lambda_l = 0;
+    vmps_gnn* gnn = nullptr;
     int cg_iters = 0;
     int cg_loop_kernels = 4, cg_nspmv = 0;
     bool ppe_pending = false;
@@ -103,6 +106,7 @@ struct mps_ctx {
     long gkernels[2] = {0, 0};
     long swaps = 0;
     double cg_relres = 0;
+    double cg_r0 = 0;  // relative residual of the CG starting point
     long steps = 0;
     bool initialized = false;
     unsigned int host_err = 0;
@@ -356,6 +360,13 @@ int vmps_bcon(mps_ctx* ctx);
 int vmps_pressure_wc(mps_ctx* ctx);
 int vmps_ppe(mps_ctx* ctx);
 int vmps_ppe_finish(mps_ctx* ctx);
+int vmps_ppe_apply(mps_ctx* ctx, const double* x, double* y);
+int vmps_gnn_guess(mps_ctx* ctx);
+int vmps_gnn_prepare(mps_ctx* ctx);
+bool vmps_gnn_in_use(const mps_ctx* ctx);
+void vmps_gnn_reset(mps_ctx* ctx);
+void vmps_gnn_free(mps_ctx* ctx);
+void vmps_drop_graphs(mps_ctx* ctx);
 void vmps_reorder_swap(mps_ctx* ctx);
 int vmps_phat(mps_ctx* ctx);
 int vmps_pressgrad(mps_ctx* ctx);

@@ -23,7 +23,9 @@ enum {
     S_BB = 0, S_RZ, S_RR, S_ZERO, S_NEWRZ, S_NEWRR, S_DONE, S_WORST,
     // mixed precision: inner r.r, its value at the sweep's start, the sweep's
     // target reduction (squared), the staged inner stop, staged inner r.r
-    S_RIN, S_RIN0, S_ETA2, S_INDONE, S_NEWRIN, S_COUNT
+    S_RIN, S_RIN0, S_ETA2, S_INDONE, S_NEWRIN,
+    S_RR0,  // r.r of the initial guess
+    S_COUNT
 };
 static_assert(S_COUNT <= 16, "cg_scal and red_host hold 16 doubles");
 constexpr int kRedThreads = 256;
@@ -314,6 +316,7 @@ __global__ void k_cg_start_scalars(int nparts, const double* __restrict__ part, 
         scal[S_BB] = bb;
         scal[S_RZ] = rz;
         scal[S_RR] = rr;
+        scal[S_RR0] = rr;
         scal[S_ZERO] = (bb == 0.0) ? 1.0 : 0.0;
         flag[0] = (bb == 0.0 || rr <= tol2 * bb) ? 1 : 0;
         flag[1] = 0;
@@ -573,6 +576,7 @@ __global__ void k_ir_start_scalars(int nparts, const double* __restrict__ part, 
         scal[S_BB] = bb;
         scal[S_RZ] = rz;
         scal[S_RR] = rr;
+        scal[S_RR0] = rr;
         scal[S_RIN] = rin;
         scal[S_RIN0] = rin;
         scal[S_ETA2] = sweep_target(tol2, bb, rr);
@@ -726,7 +730,33 @@ __global__ void k_ir_commit(double* scal, int* flag, double tol2, int use_cond,
     if (use_cond) cudaGraphSetConditional(cond, flag[0] ? 0u : 1u);
 }
 
+// y = A x on the unknown rows (0 elsewhere), with the last assembled matrix
+__global__ void k_apply(CG A, const double* __restrict__ x, double* __restrict__ y)
+{
+    Grp<32> q;
+    const long nwarps = (long)gridDim.x * blockDim.x / 32;
+    for (long w = q.gid; w < A.n; w += nwarps) {
+        const int i = (int)w;
+        double yi = 0.0;
+        if (A.bcon[i] == 0) yi = spmv_row_warp(A, q, x, i);
+        if (q.lane == 0) y[i] = yi;
+    }
+}
+
 }  // namespace
+
+// y = A x with the matrix of the last PPE (used to train the learned guess
+// on the residual it leaves)
+int vmps_ppe_apply(mps_ctx* c, const double* x, double* y)
+{
+    int sms = 0;
+    VMPS_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    CG G{c->mcol, c->mval, c->mlen, c->moff, c->diag, c->bcon, c->cap_l, c->n, 0, 0};
+    k_apply<<<sms * 8, kRedThreads, 0, c->stream>>>(G, x, y);
+    vmps_count_launch(1);
+    VMPS_CUDA(c, cudaGetLastError());
+    return MPS_OK;
+}
 
 int vmps_ppe(mps_ctx* c)
 {
@@ -746,6 +776,14 @@ int vmps_ppe(mps_ctx* c)
     A.dt = f.dt;
     A.matopt = f.matopt;
     A.srcopt = f.srcopt;
+    // learned initial guess: the network's prediction replaces the previous
+    // pressure (features are captured for training whenever a network exists)
+    int warm = f.warm_start;
+    if (c->gnn) {
+        int r = vmps_gnn_guess(c);
+        if (r != MPS_OK) return r;
+        if (vmps_gnn_in_use(c)) warm = 1;
+    }
     // CSR row offsets: exclusive scan of the Laplacian list lengths (each
     // row's non-zeros are a subset of its list)
     {
@@ -755,11 +793,11 @@ int vmps_ppe(mps_ctx* c)
     const int wblocks = (int)(((long)n * 32 + kBlock - 1) / kBlock);
     if (f.dim == 3)
         k_assemble<3><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
-                                                  nsrc, f.warm_start, c->pnew, c->pold, c->moff, c->mcol,
+                                                  nsrc, warm, c->pnew, c->pold, c->moff, c->mcol,
                                                   c->mval, c->mval32, c->mlen, c->diag, c->source);
     else
         k_assemble<2><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
-                                                  nsrc, f.warm_start, c->pnew, c->pold, c->moff, c->mcol,
+                                                  nsrc, warm, c->pnew, c->pold, c->moff, c->mcol,
                                                   c->mval, c->mval32, c->mlen, c->diag, c->source);
     vmps_count_launch(1);
     if (f.srcopt) {
@@ -937,6 +975,7 @@ int vmps_ppe_finish(mps_ctx* c)
     }
     double bb = c->red_host[S_BB], rr = c->red_host[S_RR];
     c->cg_relres = bb > 0 ? sqrt(rr / bb) : 0.0;
+    c->cg_r0 = bb > 0 ? sqrt(c->red_host[S_RR0] / bb) : 0.0;
     if (c->nscenes > 1) c->cg_relres = c->red_host[S_WORST];
     if (!(c->cg_relres <= f.cg_tol)) c->host_err |= MPS_ERR_NOT_CONVERGED;
     VMPS_CUDA(c, cudaGetLastError());
