@@ -139,9 +139,11 @@ WORKLOADS = {
        "re=2.1/4.0*l0, dt=5e-5, mixed-precision PPE (FP32 inner CG, FP64 dots and "
        "refinement) to 1e-8 relative residual",
     3: "2D two-phase dam, water 600x100 + Bingham block 150x150 (82,500 fluid), l0=0.002, "
-       "SPS-LES Cs=0.12, HB second fluid, dt=1e-4, FP64 Jacobi-PCG to 1e-8",
+       "SPS-LES Cs=0.12, HB second fluid, dt=1e-4, FP64 Jacobi-PCG to 1e-8 from the learned "
+       "initial guess (4-layer message-passing net, width 64, BF16)",
     4: "64 batched 2D dam breaks (splitmix64 seed 0, columns U[0.1,0.4]x U[0.2,0.6] m, "
-       "l0=0.005), one context, every scene's PPE to 1e-8",
+       "l0=0.005), one context, mixed-precision PPE from the learned initial guess, every "
+       "scene's PPE to 1e-8",
 }
 
 
@@ -240,10 +242,25 @@ def run_ours(args):
     mixed = cfg["precision"] == 1
     n = len(case["x"])
     fp = int((case["ptype"] > 0).sum())
+    guess = args.guess or ("learned" if args.config in (3, 4) and not args.scale else "previous")
+    trained = None
+    if guess == "learned":
+        trained = train_guess(vm, cfg, case, scenes, dev, args.gnn_train_steps)
+    if guess == "zero":
+        cfg["warm_start"] = 0
     s = vm.Solver(cfg, case, device=dev)
     if scenes is not None:
         s.set_scenes(*scenes)
     s.init()
+    if trained is not None:
+        s.gnn_create(GNN_LAYERS, 0)
+        s.gnn_params(set_to=trained["params"])
+        s.gnn_use(True)
+        # the network was fitted to the flow over the training steps: time it
+        # on the states that follow them (untimed advance, graph mode)
+        s.set_graph(bool(args.graph))
+        for _ in range(args.gnn_train_steps):
+            s.step()
     stream = torch.cuda.ExternalStream(s.stream())
 
     def barrier():
@@ -258,6 +275,7 @@ def run_ours(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         return float(t.item())
 
+    tuning = s.autotune(2) if args.autotune else s.get_tuning()
     s.set_profile(False)
     s.set_graph(bool(args.graph))
     for _ in range(args.warmup):
@@ -349,6 +367,7 @@ def run_ours(args):
                        "l2": "working set (lists, matrix) > 126 MB L2; no flush needed"},
             "fluid_particle_steps_per_s": fp * args.steps * ws / (el_ms * 1e-3),
             "graph": bool(args.graph), "ms_per_step_profiled_eager": prof_ms / args.steps,
+            "tuning": dict(tuning, autotuned=bool(args.autotune)),
             "ppe_ms_per_step": statistics.mean(ppe_ms), "cg_iters_mean": statistics.mean(iters),
             "precision": "mixed (FP32 inner CG, FP64 dots/refinement)" if mixed else "fp64",
             "cg_outer_mean": outer / args.steps,
@@ -374,11 +393,90 @@ def run_ours(args):
     s.close()
     if line is not None and mixed:
         line["error_vs_fp64"] = mixed_vs_fp64(vm, cfg, case, scenes, dev, steps=10)
+    if line is not None:
+        line["cg_guess"] = guess
+        if trained is not None:
+            line["guess_training"] = trained["info"]
+            line["advanced_steps_before_warmup"] = args.gnn_train_steps
+            line["guess_comparison"] = compare_guesses(vm, cfg, case, scenes, dev,
+                                                       trained["params"], args)
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     if line:
         print(json.dumps(line), flush=True)
+
+
+GNN_LAYERS = 4
+
+
+def train_guess(vm, cfg, case, scenes, dev, steps, iters=2, lr=2e-3):
+    """Train the learned CG initial guess online on the benchmark scene's own
+    PPE snapshots: each of `steps` solver steps (previous-pressure start) is
+    followed by `iters` Adam steps on the relative residual the network's
+    guess would have left in that step's system.  Not part of any timed
+    region; its cost is reported."""
+    import time
+    s = vm.Solver(cfg, case, device=dev)
+    if scenes is not None:
+        s.set_scenes(*scenes)
+    s.init()
+    s.gnn_create(GNN_LAYERS, 1)
+    losses = []
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s.step()
+        losses.append(s.gnn_train(iters, lr, objective="residual"))
+    sec = time.perf_counter() - t0
+    params = s.gnn_params()
+    s.close()
+    k = max(1, min(10, steps // 4))
+    return {"params": params,
+            "info": {"snapshots": steps, "adam_steps_per_snapshot": iters, "lr": lr,
+                     "objective": "|b - A x0|^2 / |b|^2 of the guess x0",
+                     "loss_first": float(sum(losses[:k]) / k),
+                     "loss_last": float(sum(losses[-k:]) / k), "seconds": sec,
+                     "network": "4 residual message-passing layers, width 64, BF16 weights "
+                                "and activations, FP32 sums"}}
+
+
+def compare_guesses(vm, cfg, case, scenes, dev, params, args, steps=20):
+    """CG iterations, initial relative residual and step time for the zero,
+    previous-pressure and learned starting points, each in a fresh context
+    advanced past the training steps, then timed over `steps` steps (graph
+    mode, CUDA events)."""
+    import torch
+    out = {}
+    for name in ("zero", "previous", "learned"):
+        c = dict(cfg)
+        c["warm_start"] = 0 if name == "zero" else 1
+        s = vm.Solver(c, case, device=dev)
+        if scenes is not None:
+            s.set_scenes(*scenes)
+        s.init()
+        if name == "learned":
+            s.gnn_create(GNN_LAYERS, 0)
+            s.gnn_params(set_to=params)
+            s.gnn_use(True)
+        s.set_graph(bool(args.graph))
+        for _ in range(args.gnn_train_steps + max(args.warmup, 3)):
+            s.step()
+        st = torch.cuda.ExternalStream(s.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        its, r0 = [], []
+        torch.cuda.synchronize()
+        e0.record(st)
+        for _ in range(steps):
+            s.step()
+            its.append(s.scalar("cg_iters"))
+            r0.append(s.scalar("cg_r0"))
+        e1.record(st)
+        torch.cuda.synchronize()
+        out[name] = {"cg_iters_mean": sum(its) / steps, "r0_rel_mean": sum(r0) / steps,
+                     "ms_per_step": e0.elapsed_time(e1) / steps}
+        s.close()
+    out["steps"] = steps
+    return out
 
 
 def mixed_vs_fp64(vm, cfg, case, scenes, dev, steps):
@@ -418,6 +516,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--graph", type=int, default=1, choices=[0, 1],
                     help="1: each step is one CUDA graph launch (CG loop as a while node)")
+    ap.add_argument("--autotune", type=int, default=1, choices=[0, 1],
+                    help="1: pick launch shapes by timing candidates on the first steps")
+    ap.add_argument("--guess", default=None, choices=["zero", "previous", "learned"],
+                    help="CG starting point (default: learned for configs 3 and 4)")
+    ap.add_argument("--gnn-train-steps", type=int, default=300,
+                    help="solver steps of online training for the learned guess")
     ap.add_argument("--precision", type=int, default=None, choices=[0, 1],
                     help="PPE precision (default: mixed for configs 2 and 4, FP64 otherwise)")
     ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2, 3, 4],

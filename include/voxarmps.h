@@ -161,6 +161,22 @@ int mps_set_profile(mps_ctx* ctx, int on);
  * identical to eager mode.  Off while profiling (mps_set_profile). */
 int mps_set_graph(mps_ctx* ctx, int on);
 
+/* ---- launch-shape autotuning (no reference counterpart) ------------------ *
+ * small_lanes: lanes per row of the PND-radius list in the list build and
+ * every stage over that list (4 or 8 in 2D, 8 or 16 in 3D; sums over a row
+ * change order with it, results stay within rounding).  cg_blocks_per_sm:
+ * grid of the CG kernels (1..8, 0 = as many as fit). */
+typedef struct mps_tuning {
+    int small_lanes;
+    int cg_blocks_per_sm;
+} mps_tuning;
+int mps_get_tuning(mps_ctx* ctx, mps_tuning* out);
+int mps_set_tuning(mps_ctx* ctx, const mps_tuning* in);
+/* Time every candidate over `steps` steps each (CUDA events, eager launches;
+ * these are real steps that advance the simulation), keep the fastest per
+ * parameter and return it.  Call it in place of the first warm-up steps. */
+int mps_autotune(mps_ctx* ctx, int steps, mps_tuning* chosen);
+
 /* ---- learned CG initial guess (no reference counterpart) ---------------- *
  * A message-passing network on the PND-radius neighbour graph (hidden width
  * 64, `layers` residual layers, BF16 weights/activations, FP32 sums) maps

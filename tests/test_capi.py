@@ -48,6 +48,21 @@ def test_config_layout_matches_c(tmp_path):
     assert int(got["SIZE"]) == C.sizeof(vm.MpsConfig)
 
 
+def test_tuning_layout_matches_c(tmp_path):
+    src = tmp_path / "tun.c"
+    fields = [n for n, _ in vm.MpsTuning._fields_]
+    body = "\n".join(f'printf("%s %zu\\n", "{f}", offsetof(mps_tuning, {f}));' for f in fields)
+    src.write_text(f'#include <stdio.h>\n#include <stddef.h>\n#include "{HEADER}"\n'
+                   f'int main(void){{ {body} printf("SIZE %zu\\n", sizeof(mps_tuning)); return 0; }}\n')
+    exe = tmp_path / "tun"
+    subprocess.run(["gcc", "-o", str(exe), str(src)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = dict(line.split() for line in out if line.strip())
+    for f in fields:
+        assert int(got[f]) == getattr(vm.MpsTuning, f).offset, f
+    assert int(got["SIZE"]) == C.sizeof(vm.MpsTuning)
+
+
 def test_missing_library_fails_loudly(tmp_path):
     with pytest.raises(RuntimeError):
         vm._LIB_SAVE = vm._LIB

@@ -46,10 +46,15 @@ EXPORTS = [
     "mps_write_vtu", "mps_stream", "mps_set_state", "mps_get_state", "mps_set_profile",
     "mps_cell_order_noalloc", "mps_set_scenes", "mps_set_graph",
     "mps_gnn_create", "mps_gnn_use", "mps_gnn_train", "mps_gnn_params", "mps_gnn_features",
-    "mps_gnn_forward", "mps_gnn_download",
+    "mps_gnn_forward", "mps_gnn_download", "mps_get_tuning", "mps_set_tuning", "mps_autotune",
 ]
 
 _LIB = None
+
+
+class MpsTuning(C.Structure):
+    """ctypes mirror of mps_tuning (include/voxarmps.h)."""
+    _fields_ = [("small_lanes", C.c_int), ("cg_blocks_per_sm", C.c_int)]
 
 
 class MpsError(RuntimeError):
@@ -93,6 +98,9 @@ def load_library(path: str = LIB_PATH):
     lib.mps_set_profile.argtypes = [P, C.c_int]
     lib.mps_set_graph.argtypes = [P, C.c_int]
     FP = C.POINTER(C.c_float)
+    lib.mps_get_tuning.argtypes = [P, C.POINTER(MpsTuning)]
+    lib.mps_set_tuning.argtypes = [P, C.POINTER(MpsTuning)]
+    lib.mps_autotune.argtypes = [P, C.c_int, C.POINTER(MpsTuning)]
     lib.mps_gnn_create.argtypes = [P, C.c_int, C.c_ulonglong]
     lib.mps_gnn_use.argtypes = [P, C.c_int]
     lib.mps_gnn_train.argtypes = [P, C.c_int, C.c_float, C.c_int, C.c_int, FP]
@@ -250,6 +258,22 @@ class Solver:
 
     def set_profile(self, on: bool = True):
         return self._chk(self.lib.mps_set_profile(self.h, int(on)), "profile")
+
+    # ---- launch-shape tuning -------------------------------------------
+    def get_tuning(self) -> dict:
+        t = MpsTuning()
+        self._chk(self.lib.mps_get_tuning(self.h, C.byref(t)), "get_tuning")
+        return {"small_lanes": t.small_lanes, "cg_blocks_per_sm": t.cg_blocks_per_sm}
+
+    def set_tuning(self, small_lanes: int, cg_blocks_per_sm: int):
+        t = MpsTuning(small_lanes, cg_blocks_per_sm)
+        return self._chk(self.lib.mps_set_tuning(self.h, C.byref(t)), "set_tuning")
+
+    def autotune(self, steps: int = 3) -> dict:
+        """Time the candidate launch shapes on real steps; keep the fastest."""
+        t = MpsTuning()
+        self._chk(self.lib.mps_autotune(self.h, steps, C.byref(t)), "autotune")
+        return {"small_lanes": t.small_lanes, "cg_blocks_per_sm": t.cg_blocks_per_sm}
 
     # ---- learned CG initial guess -------------------------------------
     def gnn_create(self, layers: int = 4, seed: int = 0):

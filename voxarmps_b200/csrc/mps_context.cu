@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <fstream>
 #include <sstream>
 #include <string>
@@ -645,6 +646,98 @@ int mps_step(mps_ctx* c)
         c->ms_stage[4] = ms;
     }
     return e | (int)(c->host_err & ~before);
+}
+
+static int small_base(const mps_ctx* c) { return c->cfg.dim == 3 ? 8 : 4; }
+
+int mps_get_tuning(mps_ctx* c, mps_tuning* out)
+{
+    if (!c || !out) return MPS_ERR_ARG;
+    out->small_lanes = small_base(c) * (c->tune_small_wide ? 2 : 1);
+    out->cg_blocks_per_sm = c->tune_cg_bps;
+    return MPS_OK;
+}
+
+int mps_set_tuning(mps_ctx* c, const mps_tuning* in)
+{
+    if (!c || !in) return MPS_ERR_ARG;
+    const int b = small_base(c);
+    if ((in->small_lanes != b && in->small_lanes != 2 * b) || in->cg_blocks_per_sm < 0 ||
+        in->cg_blocks_per_sm > 8) {
+        c->msg = "tuning: small_lanes must be the base width or twice it, cg_blocks_per_sm 0..8";
+        return MPS_ERR_ARG;
+    }
+    const int wide = in->small_lanes == 2 * b ? 1 : 0;
+    if (wide != c->tune_small_wide || in->cg_blocks_per_sm != c->tune_cg_bps) drop_graphs(c);
+    c->tune_small_wide = wide;
+    c->tune_cg_bps = in->cg_blocks_per_sm;
+    return MPS_OK;
+}
+
+// Coordinate search: the CG grid by the PPE time per CG iteration, then the
+// PND-radius lane width by the time of the rest of the step.  Each candidate
+// runs `steps` profiled steps; the median step decides.
+int mps_autotune(mps_ctx* c, int steps, mps_tuning* chosen)
+{
+    NEED_INIT(c);
+    if (steps < 1) return MPS_ERR_ARG;
+    const bool prof = c->profile;
+    TRY(mps_set_profile(c, 1));
+    auto median = [](std::vector<double> v) {
+        std::sort(v.begin(), v.end());
+        return v[v.size() / 2];
+    };
+    auto measure = [&](double* ppe_per_iter, double* rest) -> int {
+        std::vector<double> a, b;
+        for (int k = 0; k < steps; k++) {
+            int r = mps_step(c);
+            if (r & (MPS_ERR_ARG | MPS_ERR_CUDA)) return r;
+            const double its = std::max(1, c->cg_iters + c->cg_outer);
+            a.push_back(c->ms_stage[2] / its);
+            b.push_back(c->ms_stage[4] - c->ms_stage[2]);
+        }
+        *ppe_per_iter = median(a);
+        *rest = median(b);
+        return MPS_OK;
+    };
+    mps_tuning t;
+    TRY(mps_get_tuning(c, &t));
+    if (c->cfg.method != 3) {
+        int best = t.cg_blocks_per_sm;
+        double best_ms = 1e300;
+        for (int bps : {1, 2, 4, 8}) {
+            t.cg_blocks_per_sm = bps;
+            TRY(mps_set_tuning(c, &t));
+            double ppe = 0, rest = 0;
+            TRY(measure(&ppe, &rest));
+            if (ppe < best_ms) {
+                best_ms = ppe;
+                best = bps;
+            }
+        }
+        t.cg_blocks_per_sm = best;
+        TRY(mps_set_tuning(c, &t));
+    }
+    {
+        const int b = small_base(c);
+        int best = t.small_lanes;
+        double best_ms = 1e300;
+        for (int lanes : {b, 2 * b}) {
+            t.small_lanes = lanes;
+            TRY(mps_set_tuning(c, &t));
+            double ppe = 0, rest = 0;
+            TRY(measure(&ppe, &rest));
+            if (rest < best_ms) {
+                best_ms = rest;
+                best = lanes;
+            }
+        }
+        t.small_lanes = best;
+        TRY(mps_set_tuning(c, &t));
+    }
+    TRY(mps_set_profile(c, prof ? 1 : 0));
+    if (chosen) *chosen = t;
+    return MPS_OK;
 }
 
 int mps_set_graph(mps_ctx* c, int on)

@@ -96,6 +96,9 @@ struct mps_ctx {
     int cap_l = 0, cap_s = 0;
     double n0_s = 0, n0_l = 0, lambda_l = 0;
     vmps_gnn* gnn = nullptr;
+    // launch shapes picked by mps_autotune / mps_set_tuning
+    int tune_small_wide = 0;  // lanes per PND-radius row: SmallG (0) or twice that (1)
+    int tune_cg_bps = 0;      // CG grid blocks per SM (0: as many as fit, at most 8)
     int cg_iters = 0;
     int cg_loop_kernels = 4, cg_nspmv = 0;
     bool ppe_pending = false;

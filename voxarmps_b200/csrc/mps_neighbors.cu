@@ -429,20 +429,32 @@ int vmps_neighbors(mps_ctx* ctx)
                                                    ctx->P4, ctx->P4f, ctx->cell_l, ctx->cst_l,
                                                    ctx->cnt_l, nullptr, ctx->nbr_l, ctx->len_l,
                                                    ctx->len_max, 0, ctx->d_err);
-            k_lists<3, GS><<<(int)(((long)n * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
-                n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,
-                ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
-                ctx->d_err);
+            if (ctx->tune_small_wide)
+                k_lists<3, 2 * GS><<<(int)(((long)n * 2 * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+                    n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,
+                    ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
+                    ctx->d_err);
+            else
+                k_lists<3, GS><<<(int)(((long)n * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+                    n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,
+                    ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
+                    ctx->d_err);
         } else {
             constexpr int GS = SmallG<2>::G;
             k_lists<2, 32><<<n32, kBlock, 0, st>>>(n, ctx->gl, ctx->cut_l, lo_l, hi_l, ctx->cap_l,
                                                    ctx->P4, ctx->P4f, ctx->cell_l, ctx->cst_l,
                                                    ctx->cnt_l, nullptr, ctx->nbr_l, ctx->len_l,
                                                    ctx->len_max, 0, ctx->d_err);
-            k_lists<2, GS><<<(int)(((long)n * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
-                n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,
-                ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
-                ctx->d_err);
+            if (ctx->tune_small_wide)
+                k_lists<2, 2 * GS><<<(int)(((long)n * 2 * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+                    n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,
+                    ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
+                    ctx->d_err);
+            else
+                k_lists<2, GS><<<(int)(((long)n * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+                    n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,
+                    ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
+                    ctx->d_err);
         }
     }
     vmps_count_launch(2);

@@ -817,7 +817,9 @@ int vmps_ppe(mps_ctx* c)
     int nblk = 0, occ = 0;
     VMPS_CUDA(c, cudaDeviceGetAttribute(&nblk, cudaDevAttrMultiProcessorCount, c->device));
     VMPS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg_spmv, kRedThreads, 0));
-    nblk *= std::max(1, std::min(occ, 8));
+    // blocks per SM: the autotuner's choice, else as many as fit (at most 8)
+    const int bps = c->tune_cg_bps > 0 ? c->tune_cg_bps : 8;
+    nblk *= std::max(1, std::min(occ, bps));
     // layout of cg_part: [0,3*nblk) start/update partials, [4*nblk,5*nblk) p.s
     if ((size_t)5 * nblk > c->cg_part_cap) {
         c->msg = "CG partial buffer too small for the launch grid";

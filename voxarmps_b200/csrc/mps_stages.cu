@@ -719,15 +719,19 @@ Box box(mps_ctx* c)
 
 inline int group_blocks(long n, int G) { return (int)((n * G + kBlock - 1) / kBlock); }
 
-// G lanes per PND-radius row (SmallG), or a whole warp (G = 32)
+// G lanes per PND-radius row: SmallG, or twice that when the autotuner
+// chose the wide form (ctx->tune_small_wide)
 #define LAUNCH_SMALL(kern, ...)                                                           \
     do {                                                                                  \
-        if (c->cfg.dim == 3)                                                              \
-            kern<3, SmallG<3>::G><<<group_blocks(c->n, SmallG<3>::G), kBlock, 0, c->stream>>>( \
-                __VA_ARGS__);                                                             \
-        else                                                                              \
-            kern<2, SmallG<2>::G><<<group_blocks(c->n, SmallG<2>::G), kBlock, 0, c->stream>>>( \
-                __VA_ARGS__);                                                             \
+        constexpr int G3 = SmallG<3>::G, G2 = SmallG<2>::G;                               \
+        const bool wide = c->tune_small_wide != 0;                                        \
+        if (c->cfg.dim == 3) {                                                            \
+            if (wide) kern<3, 2 * G3><<<group_blocks(c->n, 2 * G3), kBlock, 0, c->stream>>>(__VA_ARGS__); \
+            else kern<3, G3><<<group_blocks(c->n, G3), kBlock, 0, c->stream>>>(__VA_ARGS__); \
+        } else {                                                                          \
+            if (wide) kern<2, 2 * G2><<<group_blocks(c->n, 2 * G2), kBlock, 0, c->stream>>>(__VA_ARGS__); \
+            else kern<2, G2><<<group_blocks(c->n, G2), kBlock, 0, c->stream>>>(__VA_ARGS__); \
+        }                                                                                 \
         vmps_count_launch(1);                                                             \
     } while (0)
 #define LAUNCH_WARP(kern, ...)                                                            \
@@ -850,12 +854,16 @@ int vmps_pressure_wc(mps_ctx* c)
 
 int vmps_phat(mps_ctx* c)
 {
-    if (c->cfg.dim == 3)
-        k_phat<SmallG<3>::G><<<group_blocks(c->n, SmallG<3>::G), kBlock, 0, c->stream>>>(
-            c->n, lists(c, 1), c->pnew, c->phat, c->PH);
+    const int G = (c->cfg.dim == 3 ? SmallG<3>::G : SmallG<2>::G) * (c->tune_small_wide ? 2 : 1);
+    if (G == 16)
+        k_phat<16><<<group_blocks(c->n, 16), kBlock, 0, c->stream>>>(c->n, lists(c, 1), c->pnew,
+                                                                     c->phat, c->PH);
+    else if (G == 8)
+        k_phat<8><<<group_blocks(c->n, 8), kBlock, 0, c->stream>>>(c->n, lists(c, 1), c->pnew,
+                                                                   c->phat, c->PH);
     else
-        k_phat<SmallG<2>::G><<<group_blocks(c->n, SmallG<2>::G), kBlock, 0, c->stream>>>(
-            c->n, lists(c, 1), c->pnew, c->phat, c->PH);
+        k_phat<4><<<group_blocks(c->n, 4), kBlock, 0, c->stream>>>(c->n, lists(c, 1), c->pnew,
+                                                                   c->phat, c->PH);
     vmps_count_launch(1);
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
