@@ -211,6 +211,21 @@ int mps_get_error(mps_ctx* ctx);
 const char* mps_last_message(mps_ctx* ctx);
 /* VTU writer (inOut.cpp:104-336 format, ASCII UnstructuredGrid). */
 int mps_write_vtu(mps_ctx* ctx, const char* path, int fluid_only);
+/* Binary VTU snapshot: VTK XML UnstructuredGrid with raw appended data
+ * (Float32 position/velocity/pressure, Int32 partType).  The state is copied
+ * device-to-host on the context's stream and the file is written by a host
+ * thread while later steps run; mps_wait_io joins that thread and returns
+ * its status.  One snapshot is in flight at a time. */
+int mps_snapshot_vtu(mps_ctx* ctx, const char* path, int fluid_only);
+int mps_wait_io(mps_ctx* ctx);
+
+/* Binary checkpoint of the full persistent state (replaces the reference's
+ * disabled VTU read-back, inOut.cpp:25-102, main.cu:393): configuration,
+ * n0, step count, every field carried between steps, scenes; checksummed.
+ * mps_load_checkpoint replaces the context's configuration and state; the
+ * resumed run continues bit for bit. */
+int mps_save_checkpoint(mps_ctx* ctx, const char* path);
+int mps_load_checkpoint(mps_ctx* ctx, const char* path);
 
 /* Device stream the context launches on (cudaStream_t as void*). */
 void* mps_stream(mps_ctx* ctx);

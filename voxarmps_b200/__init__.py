@@ -47,6 +47,7 @@ EXPORTS = [
     "mps_cell_order_noalloc", "mps_set_scenes", "mps_set_graph",
     "mps_gnn_create", "mps_gnn_use", "mps_gnn_train", "mps_gnn_params", "mps_gnn_features",
     "mps_gnn_forward", "mps_gnn_download", "mps_get_tuning", "mps_set_tuning", "mps_autotune",
+    "mps_snapshot_vtu", "mps_wait_io", "mps_save_checkpoint", "mps_load_checkpoint",
 ]
 
 _LIB = None
@@ -98,6 +99,10 @@ def load_library(path: str = LIB_PATH):
     lib.mps_set_profile.argtypes = [P, C.c_int]
     lib.mps_set_graph.argtypes = [P, C.c_int]
     FP = C.POINTER(C.c_float)
+    lib.mps_snapshot_vtu.argtypes = [P, C.c_char_p, C.c_int]
+    lib.mps_wait_io.argtypes = [P]
+    lib.mps_save_checkpoint.argtypes = [P, C.c_char_p]
+    lib.mps_load_checkpoint.argtypes = [P, C.c_char_p]
     lib.mps_get_tuning.argtypes = [P, C.POINTER(MpsTuning)]
     lib.mps_set_tuning.argtypes = [P, C.POINTER(MpsTuning)]
     lib.mps_autotune.argtypes = [P, C.c_int, C.POINTER(MpsTuning)]
@@ -258,6 +263,23 @@ class Solver:
 
     def set_profile(self, on: bool = True):
         return self._chk(self.lib.mps_set_profile(self.h, int(on)), "profile")
+
+    # ---- output and checkpoints ----------------------------------------
+    def snapshot_vtu(self, path: str, fluid_only: bool = False):
+        """Binary VTU written asynchronously (see wait_io)."""
+        return self._chk(self.lib.mps_snapshot_vtu(self.h, str(path).encode(), int(fluid_only)),
+                         "snapshot_vtu")
+
+    def wait_io(self):
+        return self._chk(self.lib.mps_wait_io(self.h), "wait_io")
+
+    def save_checkpoint(self, path: str):
+        return self._chk(self.lib.mps_save_checkpoint(self.h, str(path).encode()), "checkpoint")
+
+    def load_checkpoint(self, path: str):
+        r = self._chk(self.lib.mps_load_checkpoint(self.h, str(path).encode()), "checkpoint")
+        self.n = int(self.scalar("n"))
+        return r
 
     # ---- launch-shape tuning -------------------------------------------
     def get_tuning(self) -> dict:

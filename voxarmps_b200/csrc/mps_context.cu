@@ -67,10 +67,18 @@ void drop_graphs(mps_ctx* c)
     }
 }
 
+void snap_join(mps_ctx* c)
+{
+    if (c->snap_thread.joinable()) c->snap_thread.join();
+}
+
 void free_all(mps_ctx* c)
 {
+    snap_join(c);
     if (c->device >= 0) cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    c->snap = nullptr;  // pinned, freed below
+    c->snap_n = 0;
     drop_graphs(c);
     c->swaps = 0;
     for (void* q : c->owned) cudaFree(q);
@@ -284,7 +292,7 @@ double* field_d(mps_ctx* c, const std::string& f)
         {"wn", c->wn}, {"xs", c->xs}, {"ys", c->ys}, {"zs", c->zs}, {"us", c->us},
         {"vs", c->vs}, {"ws", c->ws}, {"n", c->nd}, {"nstar", c->nds}, {"C", c->C},
         {"meu", c->meu}, {"neut", c->neut}, {"t1", c->t1}, {"t2", c->t2}, {"t3", c->t3},
-        {"rho", c->rho}, {"source", c->source}, {"diag", c->diag}};
+        {"rho", c->rho}, {"source", c->source}, {"diag", c->diag}, {"pold", c->pold}};
     for (auto& e : t)
         if (f == e.n) return e.p;
     return nullptr;
@@ -327,11 +335,12 @@ int mps_create(const mps_config* cfg, int device, mps_ctx** out)
 int mps_destroy(mps_ctx* c)
 {
     if (!c) return MPS_OK;
-    free_all(c);
+    free_all(c);  // joins a snapshot write in flight
     vmps_gnn_free(c);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : c->ev_spmv) cudaEventDestroy(e);
+    if (c->snap_ev) cudaEventDestroy(c->snap_ev);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->stream2) cudaStreamDestroy(c->stream2);
     delete c;
@@ -821,9 +830,9 @@ int mps_download(mps_ctx* c, const char* field, void* out, long* count)
     if (double* a = field_d(c, f)) {
         k_unpermute_d<<<grid_blocks(n), kBlock, 0, st>>>(n, c->oid, a, stage);
         VMPS_CUDA(c, cudaMemcpyAsync(out, stage, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
-    } else if (f == "ptype" || f == "bcon" || f == "cell_l" || f == "cell_s") {
+    } else if (f == "ptype" || f == "bcon" || f == "cell_l" || f == "cell_s" || f == "scene") {
         const int* a = f == "ptype" ? c->ptype : f == "bcon" ? c->bcon : f == "cell_l" ? c->cell_l
-                                                                                       : c->cell_s;
+                       : f == "cell_s" ? c->cell_s : c->scene;
         k_unpermute_i<<<grid_blocks(n), kBlock, 0, st>>>(n, c->oid, a, istage);
         VMPS_CUDA(c, cudaMemcpyAsync(out, istage, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
     } else if (f == "perm_l" || f == "perm_s") {
@@ -953,6 +962,296 @@ int mps_get_error(mps_ctx* c)
 const char* mps_last_message(mps_ctx* c) { return c ? c->msg.c_str() : ""; }
 
 void* mps_stream(mps_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+
+// ------------------------------------------------------------------ checkpoints
+//
+// Binary checkpoint (replaces the reference's disabled VTU read-back,
+// inOut.cpp:25-102 / main.cu:393).  Little-endian layout:
+//   char magic[8] = "VXMPSCK1"; uint32 version = 1; uint32 config_bytes;
+//   mps_config (config_bytes); int32 n, nscenes; int64 steps;
+//   double n0_s, n0_l;
+//   15 double fields, n each, in the caller's particle order:
+//     x y z u v w p pnew phat un vn wn rho n pold
+//   int32 ptype[n], scene[n]; then, when nscenes > 1, double boxes[6 ns],
+//   pmax[ns];  uint64 FNV-1a hash of every preceding byte.
+// Resuming replays the counting sort by (cell, id) at the next step, so a
+// resumed run continues bit for bit.
+
+static const char kCkMagic[8] = {'V', 'X', 'M', 'P', 'S', 'C', 'K', '1'};
+static const char* kCkFields[15] = {"x",  "y",  "z",  "u",   "v", "w", "p", "pnew",
+                                    "phat", "un", "vn", "wn", "rho", "n", "pold"};
+
+struct Fnv {
+    unsigned long long h = 14695981039346656037ull;  // FNV-1a 64-bit offset basis
+    void add(const void* p, size_t k)
+    {
+        const unsigned char* b = (const unsigned char*)p;
+        for (size_t i = 0; i < k; i++) h = (h ^ b[i]) * 1099511628211ull;
+    }
+};
+
+int mps_save_checkpoint(mps_ctx* c, const char* path)
+{
+    NEED_INIT(c);
+    if (!path) return MPS_ERR_ARG;
+    const int n = c->n, ns = c->nscenes;
+    std::vector<double> buf((size_t)n);
+    std::vector<int> ib((size_t)n);
+    FILE* fp = fopen(path, "wb");
+    if (!fp) {
+        c->msg = std::string("cannot write ") + path;
+        return MPS_ERR_IO;
+    }
+    Fnv h;
+    bool ok = true;
+    auto put = [&](const void* p, size_t k) {
+        h.add(p, k);
+        ok = ok && fwrite(p, 1, k, fp) == k;
+    };
+    const unsigned version = 1, cb = (unsigned)sizeof(mps_config);
+    const long long steps = c->steps;
+    put(kCkMagic, 8);
+    put(&version, 4);
+    put(&cb, 4);
+    put(&c->cfg, cb);
+    put(&n, 4);
+    put(&ns, 4);
+    put(&steps, 8);
+    put(&c->n0_s, 8);
+    put(&c->n0_l, 8);
+    int r = MPS_OK;
+    for (const char* f : kCkFields) {
+        r = mps_download(c, f, buf.data(), nullptr);
+        if (r != MPS_OK) break;
+        put(buf.data(), sizeof(double) * n);
+    }
+    for (const char* f : {"ptype", "scene"}) {
+        if (r != MPS_OK) break;
+        r = mps_download(c, f, ib.data(), nullptr);
+        if (r == MPS_OK) put(ib.data(), sizeof(int) * n);
+    }
+    if (r == MPS_OK && ns > 1) {
+        std::vector<double> boxes((size_t)6 * ns), pm((size_t)ns);
+        cudaError_t e = cudaMemcpy(boxes.data(), c->sbox, sizeof(double) * 6 * ns,
+                                   cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(pm.data(), c->spmax, sizeof(double) * ns, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) r = vmps_check(c, e, "checkpoint scenes");
+        put(boxes.data(), sizeof(double) * 6 * ns);
+        put(pm.data(), sizeof(double) * ns);
+    }
+    const unsigned long long sum = h.h;
+    ok = ok && fwrite(&sum, 1, 8, fp) == 8;
+    ok = (fclose(fp) == 0) && ok;
+    if (r != MPS_OK) return r;
+    return ok ? MPS_OK : MPS_ERR_IO;
+}
+
+int mps_load_checkpoint(mps_ctx* c, const char* path)
+{
+    if (!c || !path) return MPS_ERR_ARG;
+    FILE* fp = fopen(path, "rb");
+    if (!fp) {
+        c->msg = std::string("cannot open ") + path;
+        return MPS_ERR_IO;
+    }
+    std::vector<unsigned char> all;
+    {
+        unsigned char tmp[1 << 16];
+        size_t k;
+        while ((k = fread(tmp, 1, sizeof(tmp), fp)) > 0) all.insert(all.end(), tmp, tmp + k);
+        fclose(fp);
+    }
+    size_t pos = 0;
+    auto get = [&](void* p, size_t k) {
+        if (pos + k > all.size()) return false;
+        memcpy(p, all.data() + pos, k);
+        pos += k;
+        return true;
+    };
+    auto bad = [&](const char* why) {
+        c->msg = std::string("checkpoint ") + path + ": " + why;
+        return MPS_ERR_IO;
+    };
+    if (all.size() < 8 + 8) return bad("truncated");
+    Fnv h;
+    h.add(all.data(), all.size() - 8);
+    unsigned long long sum = 0;
+    memcpy(&sum, all.data() + all.size() - 8, 8);
+    if (sum != h.h) return bad("checksum mismatch");
+    char magic[8];
+    unsigned version = 0, cb = 0;
+    if (!get(magic, 8) || memcmp(magic, kCkMagic, 8) != 0) return bad("not a checkpoint");
+    if (!get(&version, 4) || version != 1) return bad("unsupported version");
+    if (!get(&cb, 4) || cb != sizeof(mps_config)) return bad("configuration layout differs");
+    mps_config cfg;
+    int n = 0, ns = 0;
+    long long steps = 0;
+    double n0s = 0, n0l = 0;
+    if (!get(&cfg, cb) || !get(&n, 4) || !get(&ns, 4) || !get(&steps, 8) || !get(&n0s, 8) ||
+        !get(&n0l, 8) || n <= 0 || ns < 1)
+        return bad("bad header");
+    std::string why;
+    if (validate(cfg, why) != MPS_OK) return bad(why.c_str());
+    std::vector<std::vector<double>> d(15, std::vector<double>((size_t)n));
+    for (auto& a : d)
+        if (!get(a.data(), sizeof(double) * n)) return bad("truncated fields");
+    std::vector<int> pt((size_t)n), sc((size_t)n);
+    if (!get(pt.data(), sizeof(int) * n) || !get(sc.data(), sizeof(int) * n))
+        return bad("truncated fields");
+    std::vector<double> boxes, pm;
+    if (ns > 1) {
+        boxes.resize((size_t)6 * ns);
+        pm.resize((size_t)ns);
+        if (!get(boxes.data(), sizeof(double) * 6 * ns) || !get(pm.data(), sizeof(double) * ns))
+            return bad("truncated scenes");
+    }
+    c->cfg = cfg;
+    TRY(mps_upload(c, n, d[0].data(), d[1].data(), d[2].data(), pt.data(), d[3].data(),
+                   d[4].data(), d[5].data(), d[6].data()));
+    if (ns > 1) TRY(mps_set_scenes(c, ns, sc.data(), boxes.data(), pm.data()));
+    // right after the upload the slots are in caller order
+    double* dst[15] = {c->x,  c->y,  c->z,  c->u,  c->v,   c->w,  c->p,   c->pnew,
+                       c->phat, c->un, c->vn, c->wn, c->rho, c->nd, c->pold};
+    for (int k = 0; k < 15; k++)
+        VMPS_CUDA(c, cudaMemcpyAsync(dst[k], d[k].data(), sizeof(double) * n,
+                                     cudaMemcpyHostToDevice, c->stream));
+    VMPS_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->n0_s = n0s;
+    c->n0_l = n0l;
+    c->steps = steps;
+    c->initialized = true;
+    TRY(vmps_pack(c));
+    VMPS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MPS_OK;
+}
+
+// ------------------------------------------------------------------ binary VTU
+//
+// VTK XML UnstructuredGrid with raw appended data (UInt64 block headers):
+// positions and velocities as 3-component Float32 (all three components in
+// 3D), pressure Float32, partType Int32, vertex cells.  The snapshot is
+// taken on the stream (unpermute kernels + device-to-host copies into
+// pinned buffers) and written by a host thread while the device steps on;
+// mps_wait_io joins it.
+
+static int write_vtu_binary(const char* path, int n, const double* s, bool three, bool fluid_only)
+{
+    const double *x = s, *y = s + n, *z = s + 2 * (size_t)n, *u = s + 3 * (size_t)n,
+                 *v = s + 4 * (size_t)n, *w = s + 5 * (size_t)n, *p = s + 6 * (size_t)n;
+    const int* pt = (const int*)(s + 7 * (size_t)n);
+    std::vector<int> keep;
+    keep.reserve(n);
+    for (int i = 0; i < n; i++)
+        if (!fluid_only || pt[i] > 0) keep.push_back(i);
+    const unsigned long long m = keep.size();
+    std::vector<float> pos(3 * m), vel(3 * m), pr(m);
+    std::vector<int> ty(m), conn(m), offs(m);
+    std::vector<unsigned char> cell(m, 1);
+    for (size_t k = 0; k < m; k++) {
+        const int i = keep[k];
+        pos[3 * k] = (float)x[i];
+        pos[3 * k + 1] = (float)y[i];
+        pos[3 * k + 2] = three ? (float)z[i] : 0.f;
+        vel[3 * k] = (float)u[i];
+        vel[3 * k + 1] = (float)v[i];
+        vel[3 * k + 2] = three ? (float)w[i] : 0.f;
+        pr[k] = (float)p[i];
+        ty[k] = pt[i];
+        conn[k] = (int)k;
+        offs[k] = (int)k + 1;
+    }
+    struct Block { const void* p; unsigned long long bytes; };
+    Block blocks[7] = {{pos.data(), 12 * m}, {vel.data(), 12 * m}, {pr.data(), 4 * m},
+                       {ty.data(), 4 * m},   {conn.data(), 4 * m}, {offs.data(), 4 * m},
+                       {cell.data(), m}};
+    unsigned long long off[7], o = 0;
+    for (int b = 0; b < 7; b++) {
+        off[b] = o;
+        o += 8 + blocks[b].bytes;
+    }
+    FILE* fp = fopen(path, "wb");
+    if (!fp) return MPS_ERR_IO;
+    fprintf(fp, "<?xml version=\"1.0\"?>\n<VTKFile type=\"UnstructuredGrid\" version=\"1.0\" "
+                "byte_order=\"LittleEndian\" header_type=\"UInt64\">\n <UnstructuredGrid>\n"
+                "  <Piece NumberOfPoints=\"%llu\" NumberOfCells=\"%llu\">\n   <Points>\n"
+                "    <DataArray type=\"Float32\" NumberOfComponents=\"3\" Name=\"Position\" "
+                "format=\"appended\" offset=\"%llu\"/>\n   </Points>\n   <PointData>\n"
+                "    <DataArray type=\"Float32\" NumberOfComponents=\"3\" Name=\"Velocity\" "
+                "format=\"appended\" offset=\"%llu\"/>\n"
+                "    <DataArray type=\"Float32\" Name=\"Pressure\" format=\"appended\" offset=\"%llu\"/>\n"
+                "    <DataArray type=\"Int32\" Name=\"partType\" format=\"appended\" offset=\"%llu\"/>\n"
+                "   </PointData>\n   <Cells>\n"
+                "    <DataArray type=\"Int32\" Name=\"connectivity\" format=\"appended\" offset=\"%llu\"/>\n"
+                "    <DataArray type=\"Int32\" Name=\"offsets\" format=\"appended\" offset=\"%llu\"/>\n"
+                "    <DataArray type=\"UInt8\" Name=\"types\" format=\"appended\" offset=\"%llu\"/>\n"
+                "   </Cells>\n  </Piece>\n </UnstructuredGrid>\n <AppendedData encoding=\"raw\">\n_",
+            m, m, off[0], off[1], off[2], off[3], off[4], off[5], off[6]);
+    bool ok = true;
+    for (auto& b : blocks) {
+        ok = ok && fwrite(&b.bytes, 8, 1, fp) == 1;
+        if (b.bytes) ok = ok && fwrite(b.p, 1, b.bytes, fp) == b.bytes;
+    }
+    fprintf(fp, "\n </AppendedData>\n</VTKFile>\n");
+    ok = ok && !ferror(fp);
+    ok = (fclose(fp) == 0) && ok;
+    return ok ? MPS_OK : MPS_ERR_IO;
+}
+
+int mps_snapshot_vtu(mps_ctx* c, const char* path, int fluid_only)
+{
+    NEED_INIT(c);
+    if (!path) return MPS_ERR_ARG;
+    snap_join(c);  // one snapshot in flight: its buffers are reused
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    const int n = c->n;
+    if (c->snap_n < n) {
+        // 7 double fields + ptype (ints in the space of one double field)
+        double* q = nullptr;
+        VMPS_CUDA(c, cudaMallocHost(&q, sizeof(double) * 8 * (size_t)n));
+        c->pinned.push_back(q);
+        c->snap = q;
+        c->snap_n = n;
+    }
+    if (!c->snap_ev) VMPS_CUDA(c, cudaEventCreateWithFlags(&c->snap_ev, cudaEventDisableTiming));
+    cudaStream_t st = c->stream;
+    const char* names[7] = {"x", "y", "z", "u", "v", "w", "p"};
+    double* stage = c->S6;  // 6 * pitch doubles of scratch
+    for (int k = 0; k < 7; k++) {
+        double* a = field_d(c, names[k]);
+        double* slot = stage + (size_t)(k % 6) * c->pitch;
+        k_unpermute_d<<<grid_blocks(n), kBlock, 0, st>>>(n, c->oid, a, slot);
+        VMPS_CUDA(c, cudaMemcpyAsync(c->snap + (size_t)k * n, slot, sizeof(double) * n,
+                                     cudaMemcpyDeviceToHost, st));
+    }
+    int* istage = (int*)(stage + (size_t)1 * c->pitch);  // after the 7th copy was queued
+    k_unpermute_i<<<grid_blocks(n), kBlock, 0, st>>>(n, c->oid, c->ptype, istage);
+    VMPS_CUDA(c, cudaMemcpyAsync(c->snap + (size_t)7 * n, istage, sizeof(int) * n,
+                                 cudaMemcpyDeviceToHost, st));
+    vmps_count_launch(8);
+    VMPS_CUDA(c, cudaEventRecord(c->snap_ev, st));
+    const std::string file(path);
+    const bool three = c->cfg.dim == 3, fo = fluid_only != 0;
+    double* data = c->snap;
+    cudaEvent_t ev = c->snap_ev;
+    c->snap_status = MPS_OK;
+    c->snap_thread = std::thread([c, file, n, data, three, fo, ev]() {
+        if (cudaEventSynchronize(ev) != cudaSuccess) {
+            c->snap_status = MPS_ERR_CUDA;
+            return;
+        }
+        c->snap_status = write_vtu_binary(file.c_str(), n, data, three, fo);
+    });
+    return MPS_OK;
+}
+
+int mps_wait_io(mps_ctx* c)
+{
+    if (!c) return MPS_ERR_ARG;
+    snap_join(c);
+    return c->snap_status;
+}
 
 int mps_write_vtu(mps_ctx* c, const char* path, int fluid_only)
 {

@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <thread>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -186,6 +187,13 @@ struct mps_ctx {
     std::vector<void*> alts;
     std::vector<void*> owned;
     std::vector<void*> pinned;
+    // asynchronous VTU snapshots: pinned host copies (8 fields) filled by
+    // device-to-host copies on the stream, written by a host thread
+    double* snap = nullptr;
+    int snap_n = 0;
+    cudaEvent_t snap_ev = nullptr;
+    std::thread snap_thread;
+    int snap_status = 0;
 };
 
 namespace vmps {
