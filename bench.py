@@ -47,6 +47,22 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(v: float, ws: int, device: str = "cuda") -> float:
+    """Maximum of a per-rank time over all ranks (every rank gets it)."""
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: float, ws: int, ms_max: float) -> float:
+    """Units all ranks processed per second, timed by the slowest rank."""
+    return units_per_rank * ws / (ms_max * 1e-3)
+
+
 def peaks():
     try:
         with open(PEAKS_FILE) as f:
@@ -268,12 +284,8 @@ def run_ours(args):
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(v: float) -> float:
-        if ws == 1:
-            return v
-        t = torch.tensor([v], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+    def rank_max(v: float) -> float:
+        return max_over_ranks(v, ws, "cuda")
 
     tuning = s.autotune(2) if args.autotune else s.get_tuning()
     s.set_profile(False)
@@ -296,7 +308,7 @@ def run_ours(args):
     barrier()
     launches = int(s.scalar("launches") - l0)
     clocks = sampler.stop()
-    el_ms = max_over_ranks(e0.elapsed_time(e1))
+    el_ms = rank_max(e0.elapsed_time(e1))
     relres = s.scalar("cg_relres")
     # ---- the same steps again with CUDA events around every stage and
     # every SpMV launch (eager launches; events cannot sit inside the graph's
@@ -316,7 +328,7 @@ def run_ours(args):
             stage[k].append(s.scalar(k))
     p1.record(stream)
     barrier()
-    prof_ms = max_over_ranks(p0.elapsed_time(p1))
+    prof_ms = rank_max(p0.elapsed_time(p1))
     spmv_ms = s.scalar("spmv_ms")
     spmv_n = s.scalar("spmv_launches")
     nnz_a = s.scalar("nnz_a")
@@ -337,7 +349,7 @@ def run_ours(args):
         s.get_state(*ptrs)
     e3.record(stream)
     barrier()
-    e2e_ms = max_over_ranks(max(e2.elapsed_time(e3), (time.perf_counter() - t0) * 1e3))
+    e2e_ms = rank_max(max(e2.elapsed_time(e3), (time.perf_counter() - t0) * 1e3))
     bytes_state = 8 * n * len(names)
     peak, peak_kind = peaks()
     spmv_avg_ms = spmv_ms / max(spmv_n, 1)
@@ -354,7 +366,7 @@ def run_ours(args):
     if rank == 0:
         cpu = (time_reference(steps=3, warmup=1, nthreads=os.cpu_count() or 1)
                if ws == 1 and args.config in (1, 2) and not args.scale else None)
-        value = n * args.steps * ws / (el_ms * 1e-3)
+        value = whole_job_rate(n * args.steps, ws, el_ms)
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": el_ms / args.steps, "higher_is_better": True,
@@ -384,7 +396,7 @@ def run_ours(args):
                          "avg_launch_ms": spmv_avg_ms, "launches_timed": int(spmv_n),
                          "duration_source": "CUDA events around every k_cg_spmv launch "
                                             "over the K profiled steps"},
-            "e2e": {"value": n * args.steps * ws / (e2e_ms * 1e-3), "unit": METRIC,
+            "e2e": {"value": whole_job_rate(n * args.steps, ws, e2e_ms), "unit": METRIC,
                     "h2d_bytes_per_step": bytes_state, "d2h_bytes_per_step": bytes_state},
             "gpu_launches": launches, "clocks": clocks,
             "cpu_baseline": ({k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}

@@ -267,7 +267,9 @@ __device__ __forceinline__ float spmv_row_warp32(const CG& A, const float* __res
 }
 
 // r = b - A x, z = M^-1 r, p = z; partials of b.b, r.z, r.r
-__global__ void k_cg_start(CG A, const double* __restrict__ b, const double* __restrict__ x,
+// 8 resident blocks per SM (32 registers): the grid is 8 blocks per SM and
+// every block must be resident, or a second wave doubles the time
+__global__ void __launch_bounds__(256, 8) k_cg_start(CG A, const double* __restrict__ b, const double* __restrict__ x,
                            double* __restrict__ r, double* __restrict__ zv, double* __restrict__ p,
                            double* __restrict__ part)
 {
@@ -348,7 +350,7 @@ __global__ void k_cg_spmv(CG A, const double* __restrict__ p, double* __restrict
 }
 
 // alpha = rz / p.s; x += alpha p; r -= alpha s; z = M^-1 r; partials r.z, r.r
-__global__ void k_cg_update(CG A, double* __restrict__ x, double* __restrict__ r,
+__global__ void __launch_bounds__(256, 8) k_cg_update(CG A, double* __restrict__ x, double* __restrict__ r,
                             double* __restrict__ zv, const double* __restrict__ p,
                             const double* __restrict__ s, const double* __restrict__ part_ps,
                             double* __restrict__ part, const double* __restrict__ scal,
