@@ -375,7 +375,9 @@ def run_ours(args):
             "config": {"workload": (WORKLOADS[args.config] if not args.scale else
                                     f"3D dam break scaled x{args.scale} (profiling case)"),
                        "particles": n, "fluid_particles": fp,
-                       "parallelism": f"{ws} independent scenes" if ws > 1 else "1 scene",
+                       "parallelism": (f"{ws} independent replicas" if ws > 1 else "1 GPU") +
+                                      (f", {int(scenes[2].shape[0])} scenes in one context"
+                                       if scenes is not None else ""),
                        "l2": "working set (lists, matrix) > 126 MB L2; no flush needed"},
             "fluid_particle_steps_per_s": fp * args.steps * ws / (el_ms * 1e-3),
             "graph": bool(args.graph), "ms_per_step_profiled_eager": prof_ms / args.steps,
