@@ -390,8 +390,9 @@ int mps_upload(mps_ctx* c, int n, const double* x, const double* y, const double
     // FP32 screening bound: coordinates stored relative to the box minimum
     // carry an absolute error e <= extent * 2^-24 each, a difference of two
     // at most 2e + |dx| 2^-24; the squared distance of a pair near the cutoff
-    // c is off by at most sum(2|dx| de + de^2) + 3 c^2 2^-23.  The bound used
-    // is four times that, with c the larger cutoff.
+    // c is off by at most sum(2|dx| de + de^2) + 3 c^2 2^-23 (the sum of
+    // squares is formed with fused multiply-adds, at most three roundings).
+    // The bound used is four times that, with c the larger cutoff.
     {
         double ext = std::max(f.xmax - f.xmin, f.ymax - f.ymin);
         if (f.dim == 3) ext = std::max(ext, f.zmax - f.zmin);

@@ -278,7 +278,8 @@ __global__ void k_lists(int n, Grid g, double cut, float cut_lo, float cut_hi, i
                     // the screening margin [cut_lo, cut_hi]
                     float4 fj = P4f[j];
                     float ex = fj.x - fi.x, ey = fj.y - fi.y, ez = DIM == 3 ? fj.z - fi.z : 0.f;
-                    float f2 = ex * ex + ey * ey + ez * ez;
+                    // fused multiply-adds: fewer roundings than the bound assumes
+                    float f2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
                     if (f2 < cut_lo) {
                         in = (DIM == 3) || (j != i);
                     } else if (f2 <= cut_hi) {
@@ -306,6 +307,151 @@ __global__ void k_lists(int n, Grid g, double cut, float cut_lo, float cut_hi, i
         len[i] = k;
     }
 }
+
+// The same lists for Q particles of one cell at a time, one warp: each
+// candidate's packed position is loaded once and tested against the Q
+// particles, so the load, the loop and the index work are shared.  The
+// scanned ranges are the union of the Q particles' culled ranges; a range
+// a particle would have culled holds none of its neighbours, so every row
+// receives exactly the entries, in exactly the order, of the one-particle
+// kernel above.  Groups whose particles sit in different cells are done
+// one particle at a time.
+template <int DIM, int Q>
+__device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const Grid& g,
+                                          double cut, float cut_lo, float cut_hi, int cap,
+                                          const double4* __restrict__ P4,
+                                          const float4* __restrict__ P4f,
+                                          const int* __restrict__ cst, const int* __restrict__ cnt,
+                                          int* __restrict__ out, int* __restrict__ len,
+                                          int* len_max, int which, unsigned int* err)
+{
+    const int c0 = C - 1;
+    const int ic = c0 % g.ncx + 1, jc = (c0 / g.ncx) % g.ncy + 1, kc = c0 / (g.ncx * g.ncy) + 1;
+    const int m1 = (ic == 1) ? 0 : -1, m2 = (ic == g.ncx) ? 0 : 1;
+    const int m3 = (jc == 1) ? 0 : -1, m4 = (jc == g.ncy) ? 0 : 1;
+    int m5 = 0, m6 = 0;
+    if (DIM == 3) { m5 = (kc == 1) ? 0 : -1; m6 = (kc == g.ncz) ? 0 : 1; }
+    const double mx = 1e-9 * g.re, mz = 1e-9 * g.rez;
+    auto gap2 = [](int off, double lo, double hi) {
+        double d = off < 0 ? lo : (off > 0 ? hi : 0.0);
+        return d > 0 ? d * d : 0.0;
+    };
+    // union of the particles' culling decisions per (y, z) offset t:
+    // scan t unless every particle culls it; widen to x-1 / x+1 if any wants
+    unsigned scan_t = 0, lo_t = 0, hi_t = 0;
+    float4 fi[Q];
+    int k[Q];
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+        k[q] = 0;
+        if (q >= nq) continue;
+        const double4 pi = P4[i0 + q];
+        fi[q] = P4f[i0 + q];
+        const double lox = pi.x - (g.xmin + (ic - 1) * g.re) - mx;
+        const double hix = (g.xmin + ic * g.re) - pi.x - mx;
+        const double loy = pi.y - (g.ymin + (jc - 1) * g.re) - mx;
+        const double hiy = (g.ymin + jc * g.re) - pi.y - mx;
+        double loz = 0, hiz = 0;
+        if (DIM == 3) {
+            loz = pi.z - (g.zmin + (kc - 1) * g.rez) - mz;
+            hiz = (g.zmin + kc * g.rez) - pi.z - mz;
+        }
+        const double gxl = gap2(-1, lox, hix), gxh = gap2(1, lox, hix);
+        int t = 0;
+        for (int cu = m3; cu <= m4; cu++) {
+            const double gy = gap2(cu, loy, hiy);
+            for (int dp = m5; dp <= m6; dp++, t++) {
+                const double gyz = gy + (DIM == 3 ? gap2(dp, loz, hiz) : 0.0);
+                if (gyz > cut) continue;
+                scan_t |= 1u << t;
+                if (m1 < 0 && gyz + gxl <= cut) lo_t |= 1u << t;
+                if (m2 > 0 && gyz + gxh <= cut) hi_t |= 1u << t;
+            }
+        }
+    }
+    int t = 0;
+    for (int cu = m3; cu <= m4; cu++) {
+        for (int dp = m5; dp <= m6; dp++, t++) {
+            if (!(scan_t >> t & 1u)) continue;
+            const int rlo = (lo_t >> t & 1u) ? -1 : 0, rhi = (hi_t >> t & 1u) ? 1 : 0;
+            const int Cr = ic + (jc - 1 + cu) * g.ncx + (kc - 1 + dp) * g.ncx * g.ncy;
+            const int b = cst[Cr + rlo], e = cst[Cr + rhi] + cnt[Cr + rhi];
+            for (int base = b; base < e; base += 32) {
+                const int j = base + lane;
+                const bool valid = j < e;
+                const float4 fj = valid ? P4f[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for (int q = 0; q < Q; q++) {
+                    if (q >= nq) break;
+                    const int i = i0 + q;
+                    bool in = false;
+                    if (valid) {
+                        const float ex = fj.x - fi[q].x, ey = fj.y - fi[q].y,
+                                    ez = DIM == 3 ? fj.z - fi[q].z : 0.f;
+                        const float f2 =
+                            __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
+                        if (f2 < cut_lo) {
+                            in = (DIM == 3) || (j != i);
+                        } else if (f2 <= cut_hi) {
+                            const double4 pi = P4[i], pj = P4[j];
+                            const double d2 = dist2<DIM>(pj.x - pi.x, pj.y - pi.y,
+                                                         DIM == 3 ? pj.z - pi.z : 0.0);
+                            in = (DIM == 3) ? (d2 <= cut) : (j != i && d2 < cut);
+                        }
+                    }
+                    const unsigned m = __ballot_sync(0xffffffffu, in);
+                    if (in) {
+                        const int pos = k[q] + __popc(m & ((1u << lane) - 1u));
+                        if (pos < cap) out[(size_t)i * cap + pos] = j;
+                    }
+                    k[q] += __popc(m);
+                }
+            }
+        }
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+            if (q >= nq) break;
+            int kq = k[q];
+            atomicMax(&len_max[which], kq);
+            if (kq > cap) {
+                set_error(err, MPS_ERR_LIST_OVERFLOW);
+                kq = cap;
+            }
+            len[i0 + q] = kq;
+        }
+    }
+}
+
+template <int DIM, int Q>
+__global__ void k_lists_q(int n, Grid g, double cut, float cut_lo, float cut_hi, int cap,
+                          const double4* __restrict__ P4, const float4* __restrict__ P4f,
+                          const int* __restrict__ cell, const int* __restrict__ cst,
+                          const int* __restrict__ cnt, int* __restrict__ out,
+                          int* __restrict__ len, int* len_max, int which, unsigned int* err)
+{
+    const int lane = threadIdx.x & 31;
+    const long w = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w * Q >= n) return;  // whole warps leave together
+    const int i0 = (int)(w * Q);
+    const int nq = min(Q, n - i0);
+    const int C = cell[i0];
+    bool same = true;
+    for (int q = 1; q < nq; q++) same = same && cell[i0 + q] == C;
+    if (same) {
+        list_rows<DIM, Q>(lane, i0, nq, C, g, cut, cut_lo, cut_hi, cap, P4, P4f, cst, cnt, out,
+                          len, len_max, which, err);
+    } else {
+        for (int q = 0; q < nq; q++)
+            list_rows<DIM, Q>(lane, i0 + q, 1, cell[i0 + q], g, cut, cut_lo, cut_hi, cap, P4, P4f,
+                              cst, cnt, out, len, len_max, which, err);
+    }
+}
+
+// particles per warp in the Laplacian list (measured on the 1.6 M-particle
+// dam: 2 and 4 equal, 8 slower)
+constexpr int kListQ = 4;
 
 int scan(mps_ctx* ctx, int m, const int* in, int* out, int* tile_sum)
 {
@@ -418,17 +564,17 @@ int vmps_neighbors(mps_ctx* ctx)
     }
     if (ctx->profile) VMPS_CUDA(ctx, cudaEventRecord(ctx->ev[6], st));
     {
-        const int n32 = (int)(((long)n * 32 + kBlock - 1) / kBlock);
+        // Laplacian list: kListQ particles per warp
+        const int nq32 = (int)((((long)n + kListQ - 1) / kListQ * 32 + kBlock - 1) / kBlock);
         // screening window, rounded outwards to float
         auto lo = [&](double c) { return std::nextafter((float)(c - ctx->screen_abs), 0.f); };
         auto hi = [&](double c) { return std::nextafter((float)(c + ctx->screen_abs), INFINITY); };
         float lo_l = lo(ctx->cut_l), hi_l = hi(ctx->cut_l), lo_s = lo(ctx->cut_s), hi_s = hi(ctx->cut_s);
         if (ctx->cfg.dim == 3) {
             constexpr int GS = SmallG<3>::G;
-            k_lists<3, 32><<<n32, kBlock, 0, st>>>(n, ctx->gl, ctx->cut_l, lo_l, hi_l, ctx->cap_l,
-                                                   ctx->P4, ctx->P4f, ctx->cell_l, ctx->cst_l,
-                                                   ctx->cnt_l, nullptr, ctx->nbr_l, ctx->len_l,
-                                                   ctx->len_max, 0, ctx->d_err);
+            k_lists_q<3, kListQ><<<nq32, kBlock, 0, st>>>(
+                n, ctx->gl, ctx->cut_l, lo_l, hi_l, ctx->cap_l, ctx->P4, ctx->P4f, ctx->cell_l,
+                ctx->cst_l, ctx->cnt_l, ctx->nbr_l, ctx->len_l, ctx->len_max, 0, ctx->d_err);
             if (ctx->tune_small_wide)
                 k_lists<3, 2 * GS><<<(int)(((long)n * 2 * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
                     n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,
@@ -441,10 +587,9 @@ int vmps_neighbors(mps_ctx* ctx)
                     ctx->d_err);
         } else {
             constexpr int GS = SmallG<2>::G;
-            k_lists<2, 32><<<n32, kBlock, 0, st>>>(n, ctx->gl, ctx->cut_l, lo_l, hi_l, ctx->cap_l,
-                                                   ctx->P4, ctx->P4f, ctx->cell_l, ctx->cst_l,
-                                                   ctx->cnt_l, nullptr, ctx->nbr_l, ctx->len_l,
-                                                   ctx->len_max, 0, ctx->d_err);
+            k_lists_q<2, kListQ><<<nq32, kBlock, 0, st>>>(
+                n, ctx->gl, ctx->cut_l, lo_l, hi_l, ctx->cap_l, ctx->P4, ctx->P4f, ctx->cell_l,
+                ctx->cst_l, ctx->cnt_l, ctx->nbr_l, ctx->len_l, ctx->len_max, 0, ctx->d_err);
             if (ctx->tune_small_wide)
                 k_lists<2, 2 * GS><<<(int)(((long)n * 2 * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
                     n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,

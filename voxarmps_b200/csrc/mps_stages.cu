@@ -343,7 +343,7 @@ __global__ void k_predict_p(int n, Lists Ls, PredArgs A, const double4* __restri
 // PREDICTION, second part: viscous Laplacian over the Laplacian list, one
 // warp per particle, then u* and x*.
 template <int DIM>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, 5)
 k_predict(int n, Lists Ll, PredArgs A, const double* __restrict__ meu,
           const double4* __restrict__ P4, const double4* __restrict__ U4,
           const double* __restrict__ px, const double* __restrict__ py,
