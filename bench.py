@@ -287,6 +287,10 @@ def run_ours(args):
     def rank_max(v: float) -> float:
         return max_over_ranks(v, ws, "cuda")
 
+    if args.advance:  # profiling later flow states: untimed steps first
+        s.set_graph(True)
+        for _ in range(args.advance):
+            s.step()
     tuning = s.autotune(2) if args.autotune else s.get_tuning()
     s.set_profile(False)
     s.set_graph(bool(args.graph))
@@ -409,6 +413,8 @@ def run_ours(args):
         line["error_vs_fp64"] = mixed_vs_fp64(vm, cfg, case, scenes, dev, steps=10)
     if line is not None:
         line["cg_guess"] = guess
+        if args.advance:
+            line["advanced_steps_before_warmup"] = args.advance
         if trained is not None:
             line["guess_training"] = trained["info"]
             line["advanced_steps_before_warmup"] = args.gnn_train_steps
@@ -522,10 +528,17 @@ def mixed_vs_fp64(vm, cfg, case, scenes, dev, steps):
     return res
 
 
+# the run length each configuration names (configs 3 and 4 name none)
+DEFAULT_STEPS = {0: 2000, 1: 500, 2: 500, 3: 100, 4: 100}
+REF_MAX_STEPS = 20
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: the configuration's run length, "
+                         "2000 / 500 / 500 / 100 / 100 for configs 0-4)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--graph", type=int, default=1, choices=[0, 1],
@@ -540,12 +553,18 @@ def main():
                     help="PPE precision (default: mixed for configs 2 and 4, FP64 otherwise)")
     ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2, 3, 4],
                     help="benchmark configuration (1: the headline 3D dam break)")
+    ap.add_argument("--advance", type=int, default=0,
+                    help="profiling only: untimed steps before autotuning and warm-up")
     ap.add_argument("--scale", type=int, default=0,
                     help="profiling only: smaller 3D dam (10s x 20s x 10s fluid)")
     args = ap.parse_args()
     if args.impl == "reference":
+        # the reference CPU path takes ~0.75 s per step of its sample: bounded
+        args.steps = min(args.steps or 3, REF_MAX_STEPS)
         run_reference_arm(args)
     else:
+        if args.steps is None:
+            args.steps = DEFAULT_STEPS[args.config] if not args.scale else 20
         run_ours(args)
 
 
