@@ -684,15 +684,8 @@ int mps_set_tuning(mps_ctx* c, const mps_tuning* in)
     return MPS_OK;
 }
 
-// Coordinate search: the CG grid by the PPE time per CG iteration, then the
-// PND-radius lane width by the time of the rest of the step.  Each candidate
-// runs `steps` profiled steps; the median step decides.
-int mps_autotune(mps_ctx* c, int steps, mps_tuning* chosen)
+static int autotune_search(mps_ctx* c, int steps, mps_tuning& t)
 {
-    NEED_INIT(c);
-    if (steps < 1) return MPS_ERR_ARG;
-    const bool prof = c->profile;
-    TRY(mps_set_profile(c, 1));
     auto median = [](std::vector<double> v) {
         std::sort(v.begin(), v.end());
         return v[v.size() / 2];
@@ -710,8 +703,6 @@ int mps_autotune(mps_ctx* c, int steps, mps_tuning* chosen)
         *rest = median(b);
         return MPS_OK;
     };
-    mps_tuning t;
-    TRY(mps_get_tuning(c, &t));
     if (c->cfg.method != 3) {
         int best = t.cg_blocks_per_sm;
         double best_ms = 1e300;
@@ -728,24 +719,41 @@ int mps_autotune(mps_ctx* c, int steps, mps_tuning* chosen)
         t.cg_blocks_per_sm = best;
         TRY(mps_set_tuning(c, &t));
     }
-    {
-        const int b = small_base(c);
-        int best = t.small_lanes;
-        double best_ms = 1e300;
-        for (int lanes : {b, 2 * b}) {
-            t.small_lanes = lanes;
-            TRY(mps_set_tuning(c, &t));
-            double ppe = 0, rest = 0;
-            TRY(measure(&ppe, &rest));
-            if (rest < best_ms) {
-                best_ms = rest;
-                best = lanes;
-            }
-        }
-        t.small_lanes = best;
+    const int b = small_base(c);
+    int best = t.small_lanes;
+    double best_ms = 1e300;
+    for (int lanes : {b, 2 * b}) {
+        t.small_lanes = lanes;
         TRY(mps_set_tuning(c, &t));
+        double ppe = 0, rest = 0;
+        TRY(measure(&ppe, &rest));
+        if (rest < best_ms) {
+            best_ms = rest;
+            best = lanes;
+        }
     }
-    TRY(mps_set_profile(c, prof ? 1 : 0));
+    t.small_lanes = best;
+    return mps_set_tuning(c, &t);
+}
+
+// Coordinate search: the CG grid by the PPE time per CG iteration, then the
+// PND-radius lane width by the time of the rest of the step.  Each candidate
+// runs `steps` profiled steps; the median step decides.  On failure the
+// previous tuning and profiling state are restored.
+int mps_autotune(mps_ctx* c, int steps, mps_tuning* chosen)
+{
+    NEED_INIT(c);
+    if (steps < 1) return MPS_ERR_ARG;
+    const bool prof = c->profile;
+    mps_tuning before, t;
+    TRY(mps_get_tuning(c, &before));
+    t = before;
+    TRY(mps_set_profile(c, 1));
+    const int r = autotune_search(c, steps, t);
+    if (r != MPS_OK) mps_set_tuning(c, &before);
+    const int rp = mps_set_profile(c, prof ? 1 : 0);
+    if (r != MPS_OK) return r;
+    TRY(rp);
     if (chosen) *chosen = t;
     return MPS_OK;
 }

@@ -1,5 +1,7 @@
 """Readers for the solver's binary outputs (checkpoint and appended-binary
-VTU; layouts documented in include/voxarmps.h and mps_context.cu)."""
+VTU; layouts documented in include/voxarmps.h and mps_context.cu).  They
+serve tests and inspection: the checkpoint hash is checked byte by byte in
+Python, which takes seconds per hundred megabytes."""
 from __future__ import annotations
 
 import re
