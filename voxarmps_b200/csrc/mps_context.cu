@@ -238,6 +238,7 @@ int allocate(mps_ctx* c)
     TRY(dalloc(c, &c->P4c, P));
     TRY(dalloc(c, &c->U4, P));
     TRY(dalloc(c, &c->P4f, P));
+    if (c->cfg.precision == 1) TRY(dalloc(c, &c->U4f, P));
     TRY(dalloc(c, &c->PH, P));
     TRY(dalloc(c, &c->cnt_l, (size_t)c->gl.tnc + 2));
     TRY(dalloc(c, &c->cst_l, (size_t)c->gl.tnc + 2));

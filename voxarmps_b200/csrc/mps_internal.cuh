@@ -140,7 +140,8 @@ struct mps_ctx {
     // packed gathers: positions (x, y, z, ptype), predicted positions,
     // collision output, velocities (u, v, w, -) and (pnew, phat) pairs
     double4 *P4 = nullptr, *P4s = nullptr, *P4c = nullptr, *U4 = nullptr;
-    float4* P4f = nullptr;   // positions relative to the box minimum, FP32 (list screening)
+    float4* P4f = nullptr;   // positions relative to the box minimum, FP32, w = ptype
+    float4* U4f = nullptr;   // velocities, FP32 (mixed precision's viscous sums)
     double screen_abs = 0;   // bound on |d2_fp32 - d2_exact| for the screening test
     double2* PH = nullptr;
     // sort / cells
@@ -303,6 +304,42 @@ __device__ __forceinline__ double w_fast(const WK& k, double d2, double rD)
 }
 
 __device__ __forceinline__ double rsq(double d2) { return rsqrt(d2); }
+
+// W() in FP32 (mixed precision): same support tests on float thresholds
+struct WKf {
+    float re, inv_re, lt, le;
+    int ktype;
+};
+inline WKf make_wkf(const WK& k)
+{
+    return WKf{(float)k.re, (float)k.inv_re, (float)k.lt, (float)k.le, k.ktype};
+}
+template <int DIM>
+__device__ __forceinline__ float w_fast32(const WKf& k, float d2)
+{
+    const float rD = rsqrtf(d2);
+    if (k.ktype == 2) return d2 < k.lt ? k.re * rD - 1.f : 0.f;
+    const float R = d2 * rD, q = R * k.inv_re;
+    switch (k.ktype) {
+    case 6:
+        if (d2 <= k.le) {
+            const float t = 1.f - q;
+            return t * t * t;
+        }
+        return 0.f;
+    case 1:
+        if (q < 0.5f) return 2.f - 4.f * (q * q);
+        if (d2 <= k.le) {
+            const float t = 2.f * q - 2.f;
+            return t * t;
+        }
+        return 0.f;
+    case 5:
+        return d2 <= k.le ? 1.5f * logf(1.f / (q + 0.000001f)) : 0.f;
+    default:
+        return (float)kernel_w((double)R, k.ktype, DIM, (double)k.re);
+    }
+}
 
 // A group of G consecutive lanes (G divides 32) that cooperates on one row.
 template <int G>
