@@ -339,6 +339,8 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
     // union of the particles' culling decisions per (y, z) offset t:
     // scan t unless every particle culls it; widen to x-1 / x+1 if any wants
     unsigned scan_t = 0, lo_t = 0, hi_t = 0;
+    unsigned lt_mask;  // lanes below this one
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt_mask));
     float4 fi[Q];
     int k[Q];
 #pragma unroll
@@ -400,11 +402,13 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
                         }
                     }
                     const unsigned m = __ballot_sync(0xffffffffu, in);
-                    if (in) {
-                        const int pos = k[q] + __popc(m & ((1u << lane) - 1u));
-                        if (pos < cap) out[(size_t)i * cap + pos] = j;
+                    if (m) {  // warp-uniform: many batches hold no member of this particle
+                        if (in) {
+                            const int pos = k[q] + __popc(m & lt_mask);
+                            if (pos < cap) out[(size_t)i * cap + pos] = j;
+                        }
+                        k[q] += __popc(m);
                     }
-                    k[q] += __popc(m);
                 }
             }
         }
