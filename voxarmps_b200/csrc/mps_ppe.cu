@@ -29,6 +29,11 @@ enum {
 };
 static_assert(S_COUNT <= 16, "cg_scal and red_host hold 16 doubles");
 constexpr int kRedThreads = 256;
+// lanes per row, measured on the 1.6 M-particle dam: the SpMV keeps a whole
+// warp per row (16 or 8 lanes: 0.69 ms against 0.61 ms per launch); the
+// assembly runs 16 lanes per row (PPE stage 12.4 ms against 12.8 ms at 32)
+constexpr int kRowG = 32;
+constexpr int kAsmG = 16;
 
 __device__ __forceinline__ double block_sum(double v, double* sh)
 {
@@ -65,7 +70,7 @@ struct Asm {
     int matopt, srcopt;
 };
 
-// one warp per row; the non-zero columns are compacted in list order into
+// one lane group (kAsmG lanes) per row; the non-zero columns are compacted in list order into
 // the row's CSR segment (capacity = the row's list length)
 template <int DIM>
 // 6 resident blocks per SM (40 registers, a few bytes of spills): measured
@@ -79,7 +84,7 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
                            float* __restrict__ mval32, int* __restrict__ mlen,
                            double* __restrict__ diag, double* __restrict__ source)
 {
-    Grp<32> q;
+    Grp<kAsmG> q;
     int i = (int)q.gid;
     if (i >= n) return;
     int bi = bcon[i];
@@ -99,7 +104,7 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
     double* vrow = mval + moff[i];
     double dg = 0.0;
     int cnt = 0, L = len[i];
-    for (int base = 0; base < L; base += 32) {
+    for (int base = 0; base < L; base += kAsmG) {
         int k = base + q.lane;
         double v = 0.0;
         int j = -1;
@@ -215,7 +220,7 @@ struct CG {
 // plain form runs at 32 registers; restructured or deeper-unrolled variants
 // measured 15-70% slower on B200.)
 template <typename V>
-__device__ __forceinline__ double spmv_row_warp(const CG& A, const Grp<32>& q,
+__device__ __forceinline__ double spmv_row_warp(const CG& A, const Grp<kRowG>& q,
                                                 const V* __restrict__ v, int i)
 {
     const int L = A.mlen[i];
@@ -223,9 +228,9 @@ __device__ __forceinline__ double spmv_row_warp(const CG& A, const Grp<32>& q,
     const double* __restrict__ a = A.mval + A.moff[i];
     double acc0 = 0.0, acc1 = 0.0;
     int k = q.lane;
-    for (; k + 32 < L; k += 64) {
-        int c0 = __ldg(c + k), c1 = __ldg(c + k + 32);
-        double a0 = __ldg(a + k), a1 = __ldg(a + k + 32);
+    for (; k + kRowG < L; k += 2 * kRowG) {
+        int c0 = __ldg(c + k), c1 = __ldg(c + k + kRowG);
+        double a0 = __ldg(a + k), a1 = __ldg(a + k + kRowG);
         acc0 += a0 * (double)v[c0];
         acc1 += a1 * (double)v[c1];
     }
@@ -239,7 +244,7 @@ __device__ __forceinline__ double spmv_row_warp(const CG& A, const Grp<32>& q,
 // the bytes of each load, so each lane keeps four column/value pairs in
 // flight (instead of two) to hold the same bytes in flight per warp.
 __device__ __forceinline__ float spmv_row_warp32(const CG& A, const float* __restrict__ val,
-                                                 const Grp<32>& q, const float* __restrict__ v,
+                                                 const Grp<kRowG>& q, const float* __restrict__ v,
                                                  int i)
 {
     const int L = A.mlen[i];
@@ -247,19 +252,19 @@ __device__ __forceinline__ float spmv_row_warp32(const CG& A, const float* __res
     const float* __restrict__ a = val + A.moff[i];
     float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc3 = 0.f;
     int k = q.lane;
-    for (; k + 96 < L; k += 128) {
-        int c0 = __ldg(c + k), c1 = __ldg(c + k + 32), c2 = __ldg(c + k + 64),
-            c3 = __ldg(c + k + 96);
-        float a0 = __ldg(a + k), a1 = __ldg(a + k + 32), a2 = __ldg(a + k + 64),
-              a3 = __ldg(a + k + 96);
+    for (; k + 3 * kRowG < L; k += 4 * kRowG) {
+        int c0 = __ldg(c + k), c1 = __ldg(c + k + kRowG), c2 = __ldg(c + k + 2 * kRowG),
+            c3 = __ldg(c + k + 3 * kRowG);
+        float a0 = __ldg(a + k), a1 = __ldg(a + k + kRowG), a2 = __ldg(a + k + 2 * kRowG),
+              a3 = __ldg(a + k + 3 * kRowG);
         acc0 += a0 * v[c0];
         acc1 += a1 * v[c1];
         acc2 += a2 * v[c2];
         acc3 += a3 * v[c3];
     }
-    for (; k + 32 < L; k += 64) {
-        int c0 = __ldg(c + k), c1 = __ldg(c + k + 32);
-        float a0 = __ldg(a + k), a1 = __ldg(a + k + 32);
+    for (; k + kRowG < L; k += 2 * kRowG) {
+        int c0 = __ldg(c + k), c1 = __ldg(c + k + kRowG);
+        float a0 = __ldg(a + k), a1 = __ldg(a + k + kRowG);
         acc0 += a0 * v[c0];
         acc1 += a1 * v[c1];
     }
@@ -276,8 +281,8 @@ __global__ void __launch_bounds__(256, 8) k_cg_start(CG A, const double* __restr
                            double* __restrict__ part)
 {
     __shared__ double sh[33];
-    Grp<32> q;
-    const long nwarps = (long)gridDim.x * blockDim.x / 32;
+    Grp<kRowG> q;
+    const long nwarps = (long)gridDim.x * blockDim.x / kRowG;
     double bb = 0, rz = 0, rr = 0;
     for (long w = q.gid; w < A.n; w += nwarps) {
         int i = (int)w;
@@ -335,8 +340,8 @@ __global__ void k_cg_spmv(CG A, const double* __restrict__ p, double* __restrict
 {
     __shared__ double sh[33];
     if (flag[0]) return;
-    Grp<32> q;
-    const long nwarps = (long)gridDim.x * blockDim.x / 32;
+    Grp<kRowG> q;
+    const long nwarps = (long)gridDim.x * blockDim.x / kRowG;
     double ps = 0;
     for (long w = q.gid; w < A.n; w += nwarps) {
         int i = (int)w;
@@ -527,8 +532,8 @@ __global__ void k_ir_start(CG A, IR I, const double* __restrict__ b, const doubl
                            double* __restrict__ r64, double* __restrict__ part)
 {
     __shared__ double sh[33];
-    Grp<32> q;
-    const long nwarps = (long)gridDim.x * blockDim.x / 32;
+    Grp<kRowG> q;
+    const long nwarps = (long)gridDim.x * blockDim.x / kRowG;
     double bb = 0, rz = 0, rr = 0, rin = 0;
     for (long w = q.gid; w < A.n; w += nwarps) {
         int i = (int)w;
@@ -601,8 +606,8 @@ __global__ void k_ir_spmv(CG A, IR I, double* __restrict__ r64, double* __restri
     __shared__ double sh[33];
     if (flag[0]) return;
     const int phase = flag[2];
-    Grp<32> q;
-    const long nwarps = (long)gridDim.x * blockDim.x / 32;
+    Grp<kRowG> q;
+    const long nwarps = (long)gridDim.x * blockDim.x / kRowG;
     double acc = 0;
     for (long w = q.gid; w < A.n; w += nwarps) {
         int i = (int)w;
@@ -737,8 +742,8 @@ __global__ void k_ir_commit(double* scal, int* flag, double tol2, int use_cond,
 // y = A x on the unknown rows (0 elsewhere), with the last assembled matrix
 __global__ void k_apply(CG A, const double* __restrict__ x, double* __restrict__ y)
 {
-    Grp<32> q;
-    const long nwarps = (long)gridDim.x * blockDim.x / 32;
+    Grp<kRowG> q;
+    const long nwarps = (long)gridDim.x * blockDim.x / kRowG;
     for (long w = q.gid; w < A.n; w += nwarps) {
         const int i = (int)w;
         double yi = 0.0;
@@ -794,7 +799,7 @@ int vmps_ppe(mps_ctx* c)
         int r = vmps_scan(c, n, c->len_l, c->moff);
         if (r != MPS_OK) return r;
     }
-    const int wblocks = (int)(((long)n * 32 + kBlock - 1) / kBlock);
+    const int wblocks = (int)(((long)n * kAsmG + kBlock - 1) / kBlock);
     if (f.dim == 3)
         k_assemble<3><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
                                                   nsrc, warm, c->pnew, c->pold, c->moff, c->mcol,

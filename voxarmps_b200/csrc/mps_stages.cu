@@ -340,6 +340,9 @@ __global__ void k_predict_p(int n, Lists Ls, PredArgs A, const double4* __restri
     if (DIM == 3) pz[I] = pc * sum3;
 }
 
+// lanes per particle of the FP32 viscous sums (measured: 8 lanes 3.9 ms of
+// explicit stages on the 1.6 M-particle dam, 16 lanes 4.1, a warp 4.4)
+constexpr int kPred32G = 8;
 // Mixed precision: the viscous Laplacian's neighbour sums in FP32 (FP32
 // positions relative to the box, FP32 velocities, FP32 weights and sums);
 // u* and x* are then formed in FP64 exactly as in k_predict.
@@ -357,7 +360,7 @@ k_predict32(int n, Lists Ll, PredArgs A, WKf wl, const double* __restrict__ meu,
             double* __restrict__ zs, double* __restrict__ us, double* __restrict__ vs,
             double* __restrict__ ws, double4* __restrict__ P4s)
 {
-    Grp<32> q;
+    Grp<kPred32G> q;
     int I = (int)q.gid;
     if (I >= n) return;
     double4 pi = P4[I], ui4 = U4[I];
@@ -399,10 +402,10 @@ k_predict32(int n, Lists Ll, PredArgs A, WKf wl, const double* __restrict__ meu,
             s9 += dw;
         }
     };
-    // two entries per lane in flight (k, k + 32); the sums see them in list order
-    for (int k = q.lane; k < len; k += 64) {
-        const bool two = k + 32 < len;
-        const int J0 = row[k], J1 = two ? row[k + 32] : I;
+    // two entries per lane in flight (k, k + G); the sums see them in list order
+    for (int k = q.lane; k < len; k += 2 * kPred32G) {
+        const bool two = k + kPred32G < len;
+        const int J0 = row[k], J1 = two ? row[k + kPred32G] : I;
         const float4 f0 = P4f[J0], f1 = P4f[J1], v0 = U4f[J0], v1 = U4f[J1];
         add(J0, f0, v0);
         add(J1, f1, v1);
@@ -431,7 +434,10 @@ k_predict32(int n, Lists Ll, PredArgs A, WKf wl, const double* __restrict__ meu,
 }
 
 // PREDICTION, second part: viscous Laplacian over the Laplacian list, one
-// warp per particle, then u* and x*.
+// group of kPredG lanes per particle, then u* and x*.
+// lanes per particle of the viscous sums: 8 (explicit stages 5.0 ms on the
+// 1.6 M-particle dam against 5.5 ms with a whole warp; 4 is no better)
+constexpr int kPredG = 8;
 template <int DIM>
 __global__ void __launch_bounds__(256, 5)
 k_predict(int n, Lists Ll, PredArgs A, const double* __restrict__ meu,
@@ -443,7 +449,7 @@ k_predict(int n, Lists Ll, PredArgs A, const double* __restrict__ meu,
           double* __restrict__ zs, double* __restrict__ us, double* __restrict__ vs,
           double* __restrict__ ws, double4* __restrict__ P4s)
 {
-    Grp<32> q;
+    Grp<kPredG> q;
     int I = (int)q.gid;
     if (I >= n) return;
     double4 pi = P4[I], ui4 = U4[I];
@@ -462,7 +468,7 @@ k_predict(int n, Lists Ll, PredArgs A, const double* __restrict__ meu,
     double neu_same = mI / rhoI;
     const int* row = row_of(Ll, I);
     int len = Ll.len[I];
-    for (int k = q.lane; k < len; k += 32) {
+    for (int k = q.lane; k < len; k += kPredG) {
         int J = row[k];
         if (I == J) continue;
         double4 pj = P4[J];
@@ -824,6 +830,14 @@ inline int group_blocks(long n, int G) { return (int)((n * G + kBlock - 1) / kBl
         }                                                                                 \
         vmps_count_launch(1);                                                             \
     } while (0)
+#define LAUNCH_GROUP(G, kern, ...)                                                        \
+    do {                                                                                  \
+        if (c->cfg.dim == 3)                                                              \
+            kern<3><<<group_blocks(c->n, G), kBlock, 0, c->stream>>>(__VA_ARGS__);        \
+        else                                                                              \
+            kern<2><<<group_blocks(c->n, G), kBlock, 0, c->stream>>>(__VA_ARGS__);        \
+        vmps_count_launch(1);                                                             \
+    } while (0)
 #define LAUNCH_WARP(kern, ...)                                                            \
     do {                                                                                  \
         if (c->cfg.dim == 3)                                                              \
@@ -933,13 +947,13 @@ int vmps_predict(mps_ctx* c)
     LAUNCH_SMALL(k_predict_p, c->n, lists(c, 1), A, c->P4, c->pnew, c->phat, c->rho, c->pres_x,
                  c->pres_y, c->pres_z);
     if (f.precision == 1)  // FP32 neighbour sums
-        LAUNCH_WARP(k_predict32, c->n, lists(c, 0), A, make_wkf(A.wl), c->meu, c->P4, c->U4,
+        LAUNCH_GROUP(kPred32G, k_predict32, c->n, lists(c, 0), A, make_wkf(A.wl), c->meu, c->P4, c->U4,
                     c->P4f, c->U4f, c->pres_x, c->pres_y, c->pres_z, c->neut, c->t1, c->t2, c->t3,
                     c->xs, c->ys, c->zs, c->us, c->vs, c->ws, c->P4s);
     else
-        LAUNCH_WARP(k_predict, c->n, lists(c, 0), A, c->meu, c->P4, c->U4, c->pres_x, c->pres_y,
-                    c->pres_z, c->neut, c->t1, c->t2, c->t3, c->xs, c->ys, c->zs, c->us, c->vs,
-                    c->ws, c->P4s);
+        LAUNCH_GROUP(kPredG, k_predict, c->n, lists(c, 0), A, c->meu, c->P4, c->U4,
+                     c->pres_x, c->pres_y, c->pres_z, c->neut, c->t1, c->t2, c->t3, c->xs, c->ys,
+                     c->zs, c->us, c->vs, c->ws, c->P4s);
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
 }
