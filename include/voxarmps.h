@@ -163,7 +163,7 @@ int mps_set_graph(mps_ctx* ctx, int on);
 
 /* ---- launch-shape autotuning (no reference counterpart) ------------------ *
  * small_lanes: lanes per row of the PND-radius list in the list build and
- * every stage over that list (4 or 8 in 2D, 8 or 16 in 3D; sums over a row
+ * every stage over that list (4 or 8; sums over a row
  * change order with it, results stay within rounding).  cg_blocks_per_sm:
  * grid of the CG kernels (1..8, 0 = as many as fit). */
 typedef struct mps_tuning {

@@ -18,7 +18,7 @@ def test_every_shape_same_result(which):
         base = 4
     else:
         cfg, case = config.scaled_dam3d(1)
-        base = 8
+        base = 4
     cfg = gpu_cfg(cfg, cg_tol=1e-12)
     ref = None
     for lanes in (base, 2 * base):

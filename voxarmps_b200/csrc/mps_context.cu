@@ -659,7 +659,7 @@ int mps_step(mps_ctx* c)
     return e | (int)(c->host_err & ~before);
 }
 
-static int small_base(const mps_ctx* c) { return c->cfg.dim == 3 ? 8 : 4; }
+static int small_base(const mps_ctx*) { return SmallG<2>::G; }
 
 int mps_get_tuning(mps_ctx* c, mps_tuning* out)
 {

@@ -383,7 +383,10 @@ struct Grp {
 // lanes per PND-radius row
 template <int DIM>
 struct SmallG {
-    static constexpr int G = DIM == 3 ? 8 : 4;
+    // 4 lanes in 2D and 3D (3D measured: 8 lanes cost 0.8 ms more per step on
+    // the 1.6 M-particle dam, 2 lanes slow the list build); the autotuner may
+    // double it
+    static constexpr int G = 4;
 };
 
 }  // namespace vmps
