@@ -264,6 +264,8 @@ def run_ours(args):
         trained = train_guess(vm, cfg, case, scenes, dev, args.gnn_train_steps)
     if guess == "zero":
         cfg["warm_start"] = 0
+    if guess == "extrapolated":
+        cfg["warm_start"] = 2
     s = vm.Solver(cfg, case, device=dev)
     if scenes is not None:
         s.set_scenes(*scenes)
@@ -467,9 +469,9 @@ def compare_guesses(vm, cfg, case, scenes, dev, params, args, steps=20):
     mode, CUDA events)."""
     import torch
     out = {}
-    for name in ("zero", "previous", "learned"):
+    for name in ("zero", "previous", "extrapolated", "learned"):
         c = dict(cfg)
-        c["warm_start"] = 0 if name == "zero" else 1
+        c["warm_start"] = {"zero": 0, "extrapolated": 2}.get(name, 1)
         s = vm.Solver(c, case, device=dev)
         if scenes is not None:
             s.set_scenes(*scenes)
@@ -545,7 +547,7 @@ def main():
                     help="1: each step is one CUDA graph launch (CG loop as a while node)")
     ap.add_argument("--autotune", type=int, default=1, choices=[0, 1],
                     help="1: pick launch shapes by timing candidates on the first steps")
-    ap.add_argument("--guess", default=None, choices=["zero", "previous", "learned"],
+    ap.add_argument("--guess", default=None, choices=["zero", "previous", "extrapolated", "learned"],
                     help="CG starting point (default: learned for configs 3 and 4)")
     ap.add_argument("--gnn-train-steps", type=int, default=300,
                     help="solver steps of online training for the learned guess")

@@ -170,3 +170,18 @@ def test_extrapolated_initial_guess_matches_oracle():
         o.step()
     for f in ("x", "y", "u", "v", "p"):
         assert rel_err(g.get(f), o.get(f)) <= 1e-6, f
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_zero_initial_guess_matches_oracle(precision):
+    """warm_start = 0 (the reference CPU path's x0 = 0; the start kernels
+    take r = b without a product) on both sides, 6 steps, FP64 and mixed."""
+    cfg, case = config.baseline(0)
+    cfg = gpu_cfg(cfg, cg_tol=1e-12, warm_start=0, precision=precision)
+    g, o = pair(cfg, case)
+    for _ in range(6):
+        assert g.step() == 0
+        o.step()
+        assert g.scalar("cg_r0") == 1.0  # ||b - A 0|| / ||b||
+    for f in ("x", "y", "u", "v", "p"):
+        assert rel_err(g.get(f), o.get(f)) <= 1e-6, f

@@ -223,8 +223,12 @@ __global__ void k_translate(int n, const int* __restrict__ inv, const int* __res
 // stored in scan order (y, z outer, memory order inside); the reference's
 // own order (x offset outermost, ascending id per cell) is restored when
 // lists are exported (mps_download_lists).
+// 8 resident blocks per SM (32 registers, a few bytes of spills in 3D):
+// the PND-radius list stage 0.16 ms faster than at 48 registers on the
+// 1.6 M-particle dam (6 blocks: 0.08 ms; the Laplacian list's k_lists_q
+// loses at 5 blocks, its spills grow)
 template <int DIM, int G>
-__global__ void k_lists(int n, Grid g, double cut, float cut_lo, float cut_hi, int cap,
+__global__ void __launch_bounds__(256, 8) k_lists(int n, Grid g, double cut, float cut_lo, float cut_hi, int cap,
                         const double4* __restrict__ P4, const float4* __restrict__ P4f,
                         const int* __restrict__ cell, const int* __restrict__ cst,
                         const int* __restrict__ cnt, const int* __restrict__ perm,

@@ -212,6 +212,7 @@ struct CG {
     const double* __restrict__ diag;
     const int* __restrict__ bcon;
     int cap, n, precond, nparts;
+    int x0_zero;  // the initial guess is zero: r = b without a product
 };
 
 // (A v)_i with one warp on row i of the CSR matrix: coalesced column/value
@@ -292,7 +293,7 @@ __global__ void __launch_bounds__(256, 8) k_cg_start(CG A, const double* __restr
         double ri = 0, zi = 0;
         if (A.bcon[i] == 0) {
             double bi = b[i];
-            ri = bi - spmv_row_warp(A, q, x, i);
+            ri = A.x0_zero ? bi : bi - spmv_row_warp(A, q, x, i);
             zi = A.precond ? ri / A.diag[i] : ri;
             if (q.lane == 0) {
                 bb += bi * bi;
@@ -544,7 +545,7 @@ __global__ void k_ir_start(CG A, IR I, const double* __restrict__ b, const doubl
         float r32 = 0.f, z32 = 0.f;
         if (A.bcon[i] == 0) {
             double bi = b[i];
-            ri = bi - spmv_row_warp(A, q, x, i);
+            ri = A.x0_zero ? bi : bi - spmv_row_warp(A, q, x, i);
             r32 = (float)ri;
             z32 = A.precond ? r32 / (float)A.diag[i] : r32;
             if (q.lane == 0) {
@@ -763,7 +764,7 @@ int vmps_ppe_apply(mps_ctx* c, const double* x, double* y)
 {
     int sms = 0;
     VMPS_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-    CG G{c->mcol, c->mval, c->mlen, c->moff, c->diag, c->bcon, c->cap_l, c->n, 0, 0};
+    CG G{c->mcol, c->mval, c->mlen, c->moff, c->diag, c->bcon, c->cap_l, c->n, 0, 0, 0};
     k_apply<<<sms * 8, kRedThreads, 0, c->stream>>>(G, x, y);
     vmps_count_launch(1);
     VMPS_CUDA(c, cudaGetLastError());
@@ -837,8 +838,10 @@ int vmps_ppe(mps_ctx* c)
         c->msg = "CG partial buffer too small for the launch grid";
         return MPS_ERR_ARG;
     }
+    // zero initial guess (the assembly zeroed pnew): r = b exactly, so the
+    // start kernels skip the product A x0
     CG G{c->mcol, c->mval, c->mlen, c->moff, c->diag, c->bcon, c->cap_l, n,
-         f.solver == 1 ? 1 : 0, nblk};
+         f.solver == 1 ? 1 : 0, nblk, warm == 0 ? 1 : 0};
     double tol2 = f.cg_tol * f.cg_tol;
     const bool batched = c->nscenes > 1;
     // Inside a stream capture (graph mode) the loop becomes a conditional
