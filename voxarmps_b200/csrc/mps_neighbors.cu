@@ -375,47 +375,58 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
             }
         }
     }
-    int t = 0;
-    for (int cu = m3; cu <= m4; cu++) {
-        for (int dp = m5; dp <= m6; dp++, t++) {
-            if (!(scan_t >> t & 1u)) continue;
-            const int rlo = (lo_t >> t & 1u) ? -1 : 0, rhi = (hi_t >> t & 1u) ? 1 : 0;
-            const int Cr = ic + (jc - 1 + cu) * g.ncx + (kc - 1 + dp) * g.ncx * g.ncy;
-            const int b = cst[Cr + rlo], e = cst[Cr + rhi] + cnt[Cr + rhi];
-            for (int base = b; base < e; base += 32) {
-                const int j = base + lane;
-                const bool valid = j < e;
-                const float4 fj = valid ? P4f[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+    // one batch of 32 candidates against the Q particles
+    auto batch = [&](int j, bool valid, float4 fj) {
 #pragma unroll
-                for (int q = 0; q < Q; q++) {
-                    if (q >= nq) break;
-                    const int i = i0 + q;
-                    bool in = false;
-                    if (valid) {
-                        const float ex = fj.x - fi[q].x, ey = fj.y - fi[q].y,
-                                    ez = DIM == 3 ? fj.z - fi[q].z : 0.f;
-                        const float f2 =
-                            __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
-                        if (f2 < cut_lo) {
-                            in = (DIM == 3) || (j != i);
-                        } else if (f2 <= cut_hi) {
-                            const double4 pi = P4[i], pj = P4[j];
-                            const double d2 = dist2<DIM>(pj.x - pi.x, pj.y - pi.y,
-                                                         DIM == 3 ? pj.z - pi.z : 0.0);
-                            in = (DIM == 3) ? (d2 <= cut) : (j != i && d2 < cut);
-                        }
-                    }
-                    const unsigned m = __ballot_sync(0xffffffffu, in);
-                    if (m) {  // warp-uniform: many batches hold no member of this particle
-                        if (in) {
-                            const int pos = k[q] + __popc(m & lt_mask);
-                            if (pos < cap) out[(size_t)i * cap + pos] = j;
-                        }
-                        k[q] += __popc(m);
-                    }
+        for (int q = 0; q < Q; q++) {
+            if (q >= nq) break;
+            const int i = i0 + q;
+            bool in = false;
+            if (valid) {
+                const float ex = fj.x - fi[q].x, ey = fj.y - fi[q].y,
+                            ez = DIM == 3 ? fj.z - fi[q].z : 0.f;
+                const float f2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
+                if (f2 < cut_lo) {
+                    in = (DIM == 3) || (j != i);
+                } else if (f2 <= cut_hi) {
+                    const double4 pi = P4[i], pj = P4[j];
+                    const double d2 = dist2<DIM>(pj.x - pi.x, pj.y - pi.y,
+                                                 DIM == 3 ? pj.z - pi.z : 0.0);
+                    in = (DIM == 3) ? (d2 <= cut) : (j != i && d2 < cut);
                 }
             }
+            const unsigned m = __ballot_sync(0xffffffffu, in);
+            if (m) {  // warp-uniform: many batches hold no member of this particle
+                if (in) {
+                    const int pos = k[q] + __popc(m & lt_mask);
+                    if (pos < cap) out[(size_t)i * cap + pos] = j;
+                }
+                k[q] += __popc(m);
+            }
         }
+    };
+    auto scan = [&](int b, int e) {
+        for (int base = b; base < e; base += 32) {
+            const int j = base + lane;
+            const bool valid = j < e;
+            batch(j, valid, valid ? P4f[j] : make_float4(0.f, 0.f, 0.f, 0.f));
+        }
+    };
+    // the candidate range of every scanned (y, z) run, loaded at once (lane t
+    // holds run t's [b, e)) instead of one dependent load pair per run: the
+    // Laplacian list 0.11 ms faster on the 1.6 M-particle dam
+    const int ndp = m6 - m5 + 1, nt = (m4 - m3 + 1) * ndp;
+    int rb = 0, rend = 0;
+    if (lane < nt && (scan_t >> lane & 1u)) {
+        const int cu = m3 + lane / ndp, dp = m5 + lane % ndp;
+        const int rlo = (lo_t >> lane & 1u) ? -1 : 0, rhi = (hi_t >> lane & 1u) ? 1 : 0;
+        const int Cr = ic + (jc - 1 + cu) * g.ncx + (kc - 1 + dp) * g.ncx * g.ncy;
+        rb = cst[Cr + rlo];
+        rend = cst[Cr + rhi] + cnt[Cr + rhi];
+    }
+    for (int t = 0; t < nt; t++) {
+        if (!(scan_t >> t & 1u)) continue;
+        scan(__shfl_sync(0xffffffffu, rb, t), __shfl_sync(0xffffffffu, rend, t));
     }
     if (lane == 0) {
 #pragma unroll
@@ -432,8 +443,10 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
     }
 }
 
+// 4 resident blocks per SM (at most 64 registers; 66 without the bound
+// would leave 3)
 template <int DIM, int Q>
-__global__ void k_lists_q(int n, Grid g, double cut, float cut_lo, float cut_hi, int cap,
+__global__ void __launch_bounds__(256, 4) k_lists_q(int n, Grid g, double cut, float cut_lo, float cut_hi, int cap,
                           const double4* __restrict__ P4, const float4* __restrict__ P4f,
                           const int* __restrict__ cell, const int* __restrict__ cst,
                           const int* __restrict__ cnt, int* __restrict__ out,
