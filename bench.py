@@ -134,9 +134,9 @@ def spmv_algorithmic_bytes(nnz_a: float, rows: float) -> float:
 
 
 def spmv32_algorithmic_bytes(nnz_a: float, rows: float) -> float:
-    """Inner SpMV of the mixed-precision PPE: column index (4 B) and FP32
-    value (4 B) per non-zero; per row diag (8), length, offset, bcon (4 each),
-    FP32 p and s (4 each)."""
+    """Inner SpMV of the mixed-precision PPE: one (column, FP32 value) pair
+    (8 B) per non-zero; per row diag (8), length, offset, bcon (4 each), FP32
+    p and s (4 each)."""
     return nnz_a * 8.0 + rows * 28.0
 
 
@@ -402,8 +402,8 @@ def run_ours(args):
                          "traffic": traffic, "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": algo,
                          "avg_launch_ms": spmv_avg_ms, "launches_timed": int(spmv_n),
-                         "duration_source": "CUDA events around every k_cg_spmv launch "
-                                            "over the K profiled steps"},
+                         "duration_source": "CUDA events around every %s launch over the "
+                                            "K profiled steps" % ("k_ir_spmv" if mixed else "k_cg_spmv")},
             "e2e": {"value": whole_job_rate(n * args.steps, ws, e2e_ms), "unit": METRIC,
                     "h2d_bytes_per_step": bytes_state, "d2h_bytes_per_step": bytes_state},
             "gpu_launches": launches, "clocks": clocks,

@@ -252,7 +252,7 @@ int allocate(mps_ctx* c)
     TRY(dalloc(c, &c->mcol, (size_t)c->cap_l * P));
     TRY(dalloc(c, &c->mval, (size_t)c->cap_l * P));
     if (c->cfg.precision == 1) {
-        TRY(dalloc(c, &c->mval32, (size_t)c->cap_l * P));
+        TRY(dalloc(c, &c->mcv32, (size_t)c->cap_l * P));
         float** ffields[] = {&c->ir_d, &c->ir_r, &c->ir_z, &c->ir_p, &c->ir_s};
         for (auto f : ffields) TRY(dalloc(c, f, P));
     }

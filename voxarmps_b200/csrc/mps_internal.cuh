@@ -162,7 +162,7 @@ struct mps_ctx {
     double *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_s = nullptr;
     // mixed precision (precision 1): FP32 copy of the matrix values and the
     // FP32 inner-CG vectors (correction d, residual, z, direction, A p)
-    float* mval32 = nullptr;
+    int2* mcv32 = nullptr;  // mixed precision: FP32 CSR copy, (column, value bits) per entry
     float *ir_d = nullptr, *ir_r = nullptr, *ir_z = nullptr, *ir_p = nullptr, *ir_s = nullptr;
     int cg_outer = 0;
     double* cg_part = nullptr;   // block partial sums

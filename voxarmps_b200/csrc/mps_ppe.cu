@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
                            int warm, double* __restrict__ pnew, double* __restrict__ pold,
                            const int* __restrict__ moff,
                            int* __restrict__ mcol, double* __restrict__ mval,
-                           float* __restrict__ mval32, int* __restrict__ mlen,
+                           int2* __restrict__ mcv32, int* __restrict__ mlen,
                            double* __restrict__ diag, double* __restrict__ source)
 {
     Grp<kAsmG> q;
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
             int pos = cnt + __popc(m & ((1u << q.lane) - 1u));
             crow[pos] = j;
             vrow[pos] = -v;
-            if (mval32) mval32[moff[i] + pos] = (float)(-v);
+            if (mcv32) mcv32[moff[i] + pos] = make_int2(j, __float_as_int((float)(-v)));
         }
         cnt += __popc(m);
     }
@@ -244,35 +244,34 @@ __device__ __forceinline__ double spmv_row_warp(const CG& A, const Grp<kRowG>& q
 }
 
 // (A32 v)_i for the inner solve of the mixed-precision path: FP32 values,
-// FP32 products and accumulation, same warp-per-row layout.  FP32 halves
-// the bytes of each load, so each lane keeps four column/value pairs in
-// flight (instead of two) to hold the same bytes in flight per warp.
-__device__ __forceinline__ float spmv_row_warp32(const CG& A, const float* __restrict__ val,
+// FP32 products and accumulation, same warp-per-row layout.  The FP32 copy
+// interleaves each entry's column and value bits (one 8-byte load per
+// entry), and each lane keeps four entries in flight.
+__device__ __forceinline__ float spmv_row_warp32(const CG& A, const int2* __restrict__ cv,
                                                  const Grp<kRowG>& q, const float* __restrict__ v,
                                                  int i)
 {
     const int L = A.mlen[i];
-    const int* __restrict__ c = A.mcol + A.moff[i];
-    const float* __restrict__ a = val + A.moff[i];
+    const int2* __restrict__ e = cv + A.moff[i];
     float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc3 = 0.f;
     int k = q.lane;
     for (; k + 3 * kRowG < L; k += 4 * kRowG) {
-        int c0 = __ldcs(c + k), c1 = __ldcs(c + k + kRowG), c2 = __ldcs(c + k + 2 * kRowG),
-            c3 = __ldcs(c + k + 3 * kRowG);
-        float a0 = __ldcs(a + k), a1 = __ldcs(a + k + kRowG), a2 = __ldcs(a + k + 2 * kRowG),
-              a3 = __ldcs(a + k + 3 * kRowG);
-        acc0 += a0 * v[c0];
-        acc1 += a1 * v[c1];
-        acc2 += a2 * v[c2];
-        acc3 += a3 * v[c3];
+        const int2 e0 = __ldcs(e + k), e1 = __ldcs(e + k + kRowG), e2 = __ldcs(e + k + 2 * kRowG),
+                   e3 = __ldcs(e + k + 3 * kRowG);
+        acc0 += __int_as_float(e0.y) * v[e0.x];
+        acc1 += __int_as_float(e1.y) * v[e1.x];
+        acc2 += __int_as_float(e2.y) * v[e2.x];
+        acc3 += __int_as_float(e3.y) * v[e3.x];
     }
     for (; k + kRowG < L; k += 2 * kRowG) {
-        int c0 = __ldcs(c + k), c1 = __ldcs(c + k + kRowG);
-        float a0 = __ldcs(a + k), a1 = __ldcs(a + k + kRowG);
-        acc0 += a0 * v[c0];
-        acc1 += a1 * v[c1];
+        const int2 e0 = __ldcs(e + k), e1 = __ldcs(e + k + kRowG);
+        acc0 += __int_as_float(e0.y) * v[e0.x];
+        acc1 += __int_as_float(e1.y) * v[e1.x];
     }
-    if (k < L) acc2 += __ldcs(a + k) * v[__ldcs(c + k)];
+    if (k < L) {
+        const int2 e0 = __ldcs(e + k);
+        acc2 += __int_as_float(e0.y) * v[e0.x];
+    }
     float acc = q.sumf((acc0 + acc1) + (acc2 + acc3));
     return (float)A.diag[i] * v[i] + acc;
 }
@@ -512,7 +511,7 @@ __global__ void k_clamp(int n, double pmin, double pmax, const double* __restric
 // iteration, flag[2] = 1 runs a refinement; flag[1] counts inner iterations
 // and flag[3] refinements.
 struct IR {
-    const float* __restrict__ val;  // FP32 copy of the CSR values
+    const int2* __restrict__ cv;    // FP32 copy of the CSR: (column, value bits)
     float* __restrict__ d;          // correction of this sweep
     float* __restrict__ r;          // inner residual
     float* __restrict__ z;
@@ -620,7 +619,7 @@ __global__ void k_ir_spmv(CG A, IR I, double* __restrict__ r64, double* __restri
             continue;
         }
         if (phase == 0) {
-            float si = spmv_row_warp32(A, I.val, q, I.p, i);
+            float si = spmv_row_warp32(A, I.cv, q, I.p, i);
             if (q.lane == 0) {
                 I.s[i] = si;
                 acc += (double)I.p[i] * (double)si;
@@ -807,11 +806,11 @@ int vmps_ppe(mps_ctx* c)
     if (f.dim == 3)
         k_assemble<3><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
                                                   nsrc, warm, c->pnew, c->pold, c->moff, c->mcol,
-                                                  c->mval, c->mval32, c->mlen, c->diag, c->source);
+                                                  c->mval, c->mcv32, c->mlen, c->diag, c->source);
     else
         k_assemble<2><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
                                                   nsrc, warm, c->pnew, c->pold, c->moff, c->mcol,
-                                                  c->mval, c->mval32, c->mlen, c->diag, c->source);
+                                                  c->mval, c->mcv32, c->mlen, c->diag, c->source);
     vmps_count_launch(1);
     if (f.srcopt) {
         // slot of particle id k: inv_id[k] (the sort's inv buffer is free here)
@@ -853,7 +852,7 @@ int vmps_ppe(mps_ctx* c)
     cudaGraphConditionalHandle cond = 0;
     if (graph) VMPS_CUDA(c, cudaGraphConditionalHandleCreate(&cond, cgraph, 1, cudaGraphCondAssignDefault));
     const bool mixed = f.precision == 1;
-    IR I{c->mval32, c->ir_d, c->ir_r, c->ir_z, c->ir_p, c->ir_s};
+    IR I{c->mcv32, c->ir_d, c->ir_r, c->ir_z, c->ir_p, c->ir_s};
     if (mixed) {
         k_ir_start<<<nblk, kRedThreads, 0, st>>>(G, I, c->source, c->pnew, c->cg_r, c->cg_part);
         k_ir_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal,
