@@ -360,11 +360,12 @@ int mps_upload(mps_ctx* c, int n, const double* x, const double* y, const double
     c->n = n;
     c->nscenes = 1;
     c->pitch = (n + 31) / 32 * 32;
-    c->gp = c->wp = c->fp = 0;
+    c->gp = c->wp = c->fp = c->fp2 = 0;
     for (int i = 0; i < n; i++) {
         if (ptype[i] < 0) c->gp++;
         else if (ptype[i] == 0) c->wp++;
         else c->fp++;
+        if (ptype[i] == 2) c->fp2++;
     }
     if (!(f.xmin < f.xmax)) {
         // grown bounding box and PMAX of main.cu:612-715, 548

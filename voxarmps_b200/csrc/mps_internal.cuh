@@ -92,6 +92,7 @@ struct mps_ctx {
     std::string msg;
     int n = 0, pitch = 0;
     int gp = 0, wp = 0, fp = 0;
+    int fp2 = 0;  // particles of the second fluid (ptype 2)
     vmps::Grid gl{}, gs{};
     double cut_l = 0, cut_s = 0;  // squared-distance thresholds
     int cap_l = 0, cap_s = 0;

@@ -912,6 +912,12 @@ int vmps_bcon(mps_ctx* c)
 
 int vmps_vfraction(mps_ctx* c)
 {
+    // without second-fluid particles every sum2 is 0, so C = 0 everywhere
+    // (sum1 = 0 also gives 0): no neighbour pass
+    if (c->fp2 == 0) {
+        VMPS_CUDA(c, cudaMemsetAsync(c->C, 0, sizeof(double) * c->n, c->stream));
+        return MPS_OK;
+    }
     LAUNCH_SMALL(k_vfraction, c->n, lists(c, 1), c->ptype, c->P4, make_wk(c->cfg.ktype, c->cfg.re_s),
                c->cfg.fraction_method, c->C);
     VMPS_CUDA(c, cudaGetLastError());
