@@ -348,7 +348,9 @@ constexpr int kPred32G = 8;
 // Mixed precision: the viscous Laplacian's neighbour sums in FP32 (FP32
 // positions relative to the box, FP32 velocities, FP32 weights and sums);
 // u* and x* are then formed in FP64 exactly as in k_predict.
-template <int DIM>
+// TURB: the eddy-viscosity sums (sum7..9, times neut) are kept only with
+// SPS on; without it neut is 0 and they add nothing.
+template <int DIM, bool TURB>
 // 4 blocks per SM: the two-entries-in-flight loop needs the registers
 // (measured 4.4 ms explicit stages on the 1.6 M dam against 5.1 at 5 blocks)
 __global__ void __launch_bounds__(256, 4)
@@ -396,12 +398,14 @@ k_predict32(int n, Lists Ll, PredArgs A, WKf wl, const double* __restrict__ meu,
         const float du = W * (vj.x - vi.x), dv = W * (vj.y - vi.y);
         s4 += du * NEU;
         s5 += dv * NEU;
-        s7 += du;
-        s8 += dv;
+        if (TURB) {
+            s7 += du;
+            s8 += dv;
+        }
         if (DIM == 3) {
             const float dw = W * (vj.z - vi.z);
             s6 += dw * NEU;
-            s9 += dw;
+            if (TURB) s9 += dw;
         }
     };
     // two entries per lane in flight (k, k + G); the sums see them in list order
@@ -412,11 +416,13 @@ k_predict32(int n, Lists Ll, PredArgs A, WKf wl, const double* __restrict__ meu,
         add(J0, f0, v0);
         add(J1, f1, v1);
     }
-    double sum4 = q.sum((double)s4), sum5 = q.sum((double)s5), sum7 = q.sum((double)s7),
-           sum8 = q.sum((double)s8), sum6 = 0, sum9 = 0;
-    if (DIM == 3) { sum6 = q.sum((double)s6); sum9 = q.sum((double)s9); }
+    double sum4 = q.sum((double)s4), sum5 = q.sum((double)s5), sum7 = 0, sum8 = 0, sum6 = 0,
+           sum9 = 0;
+    if (TURB) { sum7 = q.sum((double)s7); sum8 = q.sum((double)s8); }
+    if (DIM == 3) sum6 = q.sum((double)s6);
+    if (DIM == 3 && TURB) sum9 = q.sum((double)s9);
     if (q.lane != 0) return;
-    double DT = A.dt, nt = neut[I];
+    double DT = A.dt, nt = TURB ? neut[I] : 0.0;
     double uS = ui4.x + A.gx * DT + A.visc_coef * (sum4 + nt * sum7) + DT * t1[I] - px[I];
     double vS = ui4.y + A.gy * DT + A.visc_coef * (sum5 + nt * sum8) + DT * t2[I] - py[I];
     double4 o = pi;
@@ -440,7 +446,10 @@ k_predict32(int n, Lists Ll, PredArgs A, WKf wl, const double* __restrict__ meu,
 // lanes per particle of the viscous sums: 8 (explicit stages 5.0 ms on the
 // 1.6 M-particle dam against 5.5 ms with a whole warp; 4 is no better)
 constexpr int kPredG = 8;
-template <int DIM>
+// TURB: the eddy-viscosity sums (sum7..9, times neut) are kept only with
+// SPS on; without it neut is 0 and they add nothing (explicit stages 0.19
+// ms faster on the 1.6 M-particle dam; 6 blocks per SM at 40 registers lose)
+template <int DIM, bool TURB>
 __global__ void __launch_bounds__(256, 5)
 k_predict(int n, Lists Ll, PredArgs A, const double* __restrict__ meu,
           const double4* __restrict__ P4, const double4* __restrict__ U4,
@@ -487,18 +496,22 @@ k_predict(int n, Lists Ll, PredArgs A, const double* __restrict__ meu,
         double du = W * (uj.x - ui4.x), dv = W * (uj.y - ui4.y);
         sum4 += du * NEU;
         sum5 += dv * NEU;
-        sum7 += du;
-        sum8 += dv;
+        if (TURB) {
+            sum7 += du;
+            sum8 += dv;
+        }
         if (DIM == 3) {
             double dw = W * (uj.z - ui4.z);
             sum6 += dw * NEU;
-            sum9 += dw;
+            if (TURB) sum9 += dw;
         }
     }
-    sum4 = q.sum(sum4); sum5 = q.sum(sum5); sum7 = q.sum(sum7); sum8 = q.sum(sum8);
-    if (DIM == 3) { sum6 = q.sum(sum6); sum9 = q.sum(sum9); }
+    sum4 = q.sum(sum4); sum5 = q.sum(sum5);
+    if (TURB) { sum7 = q.sum(sum7); sum8 = q.sum(sum8); }
+    if (DIM == 3) sum6 = q.sum(sum6);
+    if (DIM == 3 && TURB) sum9 = q.sum(sum9);
     if (q.lane != 0) return;
-    double DT = A.dt, nt = neut[I];
+    double DT = A.dt, nt = TURB ? neut[I] : 0.0;
     double uS = ui4.x + A.gx * DT + A.visc_coef * (sum4 + nt * sum7) + DT * t1[I] - px[I];
     double vS = ui4.y + A.gy * DT + A.visc_coef * (sum5 + nt * sum8) + DT * t2[I] - py[I];
     double4 o = pi;
@@ -955,14 +968,27 @@ int vmps_predict(mps_ctx* c)
     A.rho1 = f.rho1; A.rho2 = f.rho2;
     LAUNCH_SMALL(k_predict_p, c->n, lists(c, 1), A, c->P4, c->pnew, c->phat, c->rho, c->pres_x,
                  c->pres_y, c->pres_z);
-    if (f.precision == 1)  // FP32 neighbour sums
-        LAUNCH_GROUP(kPred32G, k_predict32, c->n, lists(c, 0), A, make_wkf(A.wl), c->meu, c->P4, c->U4,
-                    c->P4f, c->U4f, c->pres_x, c->pres_y, c->pres_z, c->neut, c->t1, c->t2, c->t3,
-                    c->xs, c->ys, c->zs, c->us, c->vs, c->ws, c->P4s);
-    else
-        LAUNCH_GROUP(kPredG, k_predict, c->n, lists(c, 0), A, c->meu, c->P4, c->U4,
-                     c->pres_x, c->pres_y, c->pres_z, c->neut, c->t1, c->t2, c->t3, c->xs, c->ys,
-                     c->zs, c->us, c->vs, c->ws, c->P4s);
+    // without SPS, neut is 0 and the eddy-viscosity sums are left out
+#define PRED32(D, T)                                                                          \
+    k_predict32<D, T><<<group_blocks(c->n, kPred32G), kBlock, 0, c->stream>>>(                 \
+        c->n, lists(c, 0), A, make_wkf(A.wl), c->meu, c->P4, c->U4, c->P4f, c->U4f, c->pres_x, \
+        c->pres_y, c->pres_z, c->neut, c->t1, c->t2, c->t3, c->xs, c->ys, c->zs, c->us, c->vs,  \
+        c->ws, c->P4s)
+#define PRED64(D, T)                                                                          \
+    k_predict<D, T><<<group_blocks(c->n, kPredG), kBlock, 0, c->stream>>>(                     \
+        c->n, lists(c, 0), A, c->meu, c->P4, c->U4, c->pres_x, c->pres_y, c->pres_z, c->neut,  \
+        c->t1, c->t2, c->t3, c->xs, c->ys, c->zs, c->us, c->vs, c->ws, c->P4s)
+    const bool turb = f.turb != 0;
+    if (f.precision == 1) {  // FP32 neighbour sums
+        if (f.dim == 3) { if (turb) PRED32(3, true); else PRED32(3, false); }
+        else { if (turb) PRED32(2, true); else PRED32(2, false); }
+    } else {
+        if (f.dim == 3) { if (turb) PRED64(3, true); else PRED64(3, false); }
+        else { if (turb) PRED64(2, true); else PRED64(2, false); }
+    }
+#undef PRED32
+#undef PRED64
+    vmps_count_launch(1);
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
 }
