@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
                            const int* __restrict__ moff,
                            int* __restrict__ mcol, double* __restrict__ mval,
                            int2* __restrict__ mcv32, int* __restrict__ mlen,
-                           double* __restrict__ diag, double* __restrict__ source)
+                           double* __restrict__ diag, double* __restrict__ source, int w_bcon)
 {
     Grp<kAsmG> q;
     int i = (int)q.gid;
@@ -111,9 +111,16 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
         bool keep = false;
         if (k < L) {
             j = row[k];
-            int bj = j == i ? -1 : bcon[j];
+            double4 pj;
+            int bj;
+            if (w_bcon) {  // P4's w slot holds bcon: one gather
+                pj = P4[j];
+                bj = j == i ? -1 : (int)pj.w;
+            } else {
+                bj = j == i ? -1 : bcon[j];
+                if (bj != -1) pj = P4[j];
+            }
             if (bj != -1) {
-                double4 pj = P4[j];
                 double d2 = dist2<DIM>(pj.x - pi.x, pj.y - pi.y, DIM == 3 ? pj.z - pi.z : 0.0);
                 if (d2 > A.tiny2) {
                     double rD = rsq(d2);
@@ -803,14 +810,18 @@ int vmps_ppe(mps_ctx* c)
         if (r != MPS_OK) return r;
     }
     const int wblocks = (int)(((long)n * kAsmG + kBlock - 1) / kBlock);
+    // the predicted positions carry bcon in their w slot (written by BCON)
+    const int w_bcon = f.ppe_at_predicted ? 1 : 0;
     if (f.dim == 3)
         k_assemble<3><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
                                                   nsrc, warm, c->pnew, c->pold, c->moff, c->mcol,
-                                                  c->mval, c->mcv32, c->mlen, c->diag, c->source);
+                                                  c->mval, c->mcv32, c->mlen, c->diag, c->source,
+                                                  w_bcon);
     else
         k_assemble<2><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
                                                   nsrc, warm, c->pnew, c->pold, c->moff, c->mcol,
-                                                  c->mval, c->mcv32, c->mlen, c->diag, c->source);
+                                                  c->mval, c->mcv32, c->mlen, c->diag, c->source,
+                                                  w_bcon);
     vmps_count_launch(1);
     if (f.srcopt) {
         // slot of particle id k: inv_id[k] (the sort's inv buffer is free here)

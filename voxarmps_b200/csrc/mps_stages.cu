@@ -74,8 +74,12 @@ __global__ void k_pnd(int n, Lists L, const double4* __restrict__ P4, WK wk, int
 }
 
 // BCON (functions.cu:433-445)
+// P4w (the predicted positions the PPE is assembled at, or null): its w
+// slot, unread after PNUMSTAR, takes bcon so that the assembly finds each
+// neighbour's position and status in one gather
 __global__ void k_bcon(int n, const int* __restrict__ ptype, const double* __restrict__ nd,
-                       double n0, double dirichlet, int* __restrict__ bcon)
+                       double n0, double dirichlet, int* __restrict__ bcon,
+                       double4* __restrict__ P4w)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -84,6 +88,7 @@ __global__ void k_bcon(int n, const int* __restrict__ ptype, const double* __res
     else if (nd[i] / n0 < dirichlet) b = 1;
     else b = 0;
     bcon[i] = b;
+    if (P4w) reinterpret_cast<double*>(P4w + i)[3] = (double)b;
 }
 
 // V_FRACTION (functions.cu:2580-2638)
@@ -683,8 +688,10 @@ struct CollArgs {
 // from the pre-collision state.  The position and velocity changes go to the
 // delta arrays; k_collision_apply adds them once every particle has read the
 // pre-collision state (no buffer swap, so the step's buffers stay fixed).
+// 4 resident blocks per SM (64 registers, 28 bytes of spills; 80 without the
+// bound): 0.02 ms per step faster on the 1.6 M-particle dam.
 template <int DIM, int G>
-__global__ void k_collision(int n, Lists L, CollArgs A, const int* __restrict__ ptype,
+__global__ void __launch_bounds__(256, 4) k_collision(int n, Lists L, CollArgs A, const int* __restrict__ ptype,
                             const double4* __restrict__ P4, const double* __restrict__ un,
                             const double* __restrict__ vn, const double* __restrict__ wn,
                             double* __restrict__ dxo, double* __restrict__ dyo,
@@ -916,8 +923,9 @@ int vmps_pnd(mps_ctx* c, int at_star, int correct, int which, double* out)
 
 int vmps_bcon(mps_ctx* c)
 {
-    k_bcon<<<grid_blocks(c->n), kBlock, 0, c->stream>>>(c->n, c->ptype, c->nds, c->n0_s,
-                                                        c->cfg.dirichlet, c->bcon);
+    k_bcon<<<grid_blocks(c->n), kBlock, 0, c->stream>>>(
+        c->n, c->ptype, c->nds, c->n0_s, c->cfg.dirichlet, c->bcon,
+        c->cfg.ppe_at_predicted ? c->P4s : nullptr);
     vmps_count_launch(1);
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
