@@ -361,6 +361,7 @@ int mps_upload(mps_ctx* c, int n, const double* x, const double* y, const double
     c->nscenes = 1;
     c->pitch = (n + 31) / 32 * 32;
     c->gp = c->wp = c->fp = c->fp2 = 0;
+    c->p4s_bcon = false;
     for (int i = 0; i < n; i++) {
         if (ptype[i] < 0) c->gp++;
         else if (ptype[i] == 0) c->wp++;

@@ -93,6 +93,7 @@ struct mps_ctx {
     int n = 0, pitch = 0;
     int gp = 0, wp = 0, fp = 0;
     int fp2 = 0;  // particles of the second fluid (ptype 2)
+    bool p4s_bcon = false;  // P4s.w holds bcon (BCON ran after the last PREDICTION)
     vmps::Grid gl{}, gs{};
     double cut_l = 0, cut_s = 0;  // squared-distance thresholds
     int cap_l = 0, cap_s = 0;

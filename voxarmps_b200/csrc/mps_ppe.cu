@@ -810,8 +810,10 @@ int vmps_ppe(mps_ctx* c)
         if (r != MPS_OK) return r;
     }
     const int wblocks = (int)(((long)n * kAsmG + kBlock - 1) / kBlock);
-    // the predicted positions carry bcon in their w slot (written by BCON)
-    const int w_bcon = f.ppe_at_predicted ? 1 : 0;
+    // the predicted positions carry bcon in their w slot when BCON ran after
+    // the last PREDICTION (always within a step; the per-stage entry points
+    // may be called out of order)
+    const int w_bcon = (f.ppe_at_predicted && c->p4s_bcon) ? 1 : 0;
     if (f.dim == 3)
         k_assemble<3><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
                                                   nsrc, warm, c->pnew, c->pold, c->moff, c->mcol,

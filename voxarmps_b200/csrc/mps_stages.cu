@@ -926,6 +926,7 @@ int vmps_bcon(mps_ctx* c)
     k_bcon<<<grid_blocks(c->n), kBlock, 0, c->stream>>>(
         c->n, c->ptype, c->nds, c->n0_s, c->cfg.dirichlet, c->bcon,
         c->cfg.ppe_at_predicted ? c->P4s : nullptr);
+    c->p4s_bcon = c->cfg.ppe_at_predicted != 0;
     vmps_count_launch(1);
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
@@ -987,6 +988,7 @@ int vmps_predict(mps_ctx* c)
         c->n, lists(c, 0), A, c->meu, c->P4, c->U4, c->pres_x, c->pres_y, c->pres_z, c->neut,  \
         c->t1, c->t2, c->t3, c->xs, c->ys, c->zs, c->us, c->vs, c->ws, c->P4s)
     const bool turb = f.turb != 0;
+    c->p4s_bcon = false;  // P4s.w is ptype again until BCON
     if (f.precision == 1) {  // FP32 neighbour sums
         if (f.dim == 3) { if (turb) PRED32(3, true); else PRED32(3, false); }
         else { if (turb) PRED32(2, true); else PRED32(2, false); }
