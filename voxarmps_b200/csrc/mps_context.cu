@@ -249,6 +249,7 @@ int allocate(mps_ctx* c)
     // row-major lists and matrix: row i at i * cap
     TRY(dalloc(c, &c->nbr_l, (size_t)c->cap_l * P));
     TRY(dalloc(c, &c->nbr_s, (size_t)c->cap_s * P));
+    TRY(dalloc(c, &c->mrow, P));
     TRY(dalloc(c, &c->mcol, (size_t)c->cap_l * P));
     TRY(dalloc(c, &c->mval, (size_t)c->cap_l * P));
     if (c->cfg.precision == 1) {

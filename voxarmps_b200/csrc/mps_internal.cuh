@@ -159,6 +159,7 @@ struct mps_ctx {
     int *nbr_l = nullptr, *len_l = nullptr, *nbr_s = nullptr, *len_s = nullptr;
     // PPE matrix (compact slot-major ELL) and CG vectors
     int *mcol = nullptr, *mlen = nullptr, *moff = nullptr;  // CSR: row i at moff[i]
+    int2* mrow = nullptr;  // (moff, mlen) per row, mlen -1 for rows outside the system
     double* mval = nullptr;
     double *pres_x = nullptr, *pres_y = nullptr, *pres_z = nullptr;  // prediction pressure sums
     double *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_s = nullptr;

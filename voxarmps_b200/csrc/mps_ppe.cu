@@ -82,7 +82,8 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
                            const int* __restrict__ moff,
                            int* __restrict__ mcol, double* __restrict__ mval,
                            int2* __restrict__ mcv32, int* __restrict__ mlen,
-                           double* __restrict__ diag, double* __restrict__ source, int w_bcon)
+                           double* __restrict__ diag, double* __restrict__ source, int w_bcon,
+                           int2* __restrict__ mrow)
 {
     Grp<kAsmG> q;
     int i = (int)q.gid;
@@ -91,6 +92,7 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
     if (bi != 0) {
         if (q.lane == 0) {
             mlen[i] = 0;
+            mrow[i] = make_int2(moff[i], -1);
             diag[i] = 0.0;
             source[i] = 0.0;
             if (warm == 2) pold[i] = pnew[i];
@@ -143,6 +145,7 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
     if (q.lane == 0) {
         diag[i] = dg + A.reg;
         mlen[i] = cnt;
+        mrow[i] = make_int2(moff[i], cnt);
         if (!A.srcopt) source[i] = 1.0 / A.dt / A.dt * (nsrc[i] - A.n0_s) / A.n0_s;
         // initial guess: 0, the previous pressure, or the linear extrapolation
         // 2 p^n - p^(n-1) (pold keeps p^n for the next step)
@@ -220,6 +223,7 @@ struct CG {
     const int* __restrict__ bcon;
     int cap, n, precond, nparts;
     int x0_zero;  // the initial guess is zero: r = b without a product
+    const int2* __restrict__ mrow;  // (offset, length) per row; length -1: not an unknown
 };
 
 // (A v)_i with one warp on row i of the CSR matrix: coalesced column/value
@@ -231,12 +235,11 @@ struct CG {
 // gathered vector in L1/L2: 0.61 against 0.755 ms per launch after 700 steps
 // of the 1.6 M-particle dam, equal on its first steps.
 template <typename V>
-__device__ __forceinline__ double spmv_row_warp(const CG& A, const Grp<kRowG>& q,
-                                                const V* __restrict__ v, int i)
+__device__ __forceinline__ double spmv_row(const CG& A, const Grp<kRowG>& q,
+                                           const V* __restrict__ v, int i, int off, int L)
 {
-    const int L = A.mlen[i];
-    const int* __restrict__ c = A.mcol + A.moff[i];
-    const double* __restrict__ a = A.mval + A.moff[i];
+    const int* __restrict__ c = A.mcol + off;
+    const double* __restrict__ a = A.mval + off;
     double acc0 = 0.0, acc1 = 0.0;
     int k = q.lane;
     for (; k + kRowG < L; k += 2 * kRowG) {
@@ -248,6 +251,13 @@ __device__ __forceinline__ double spmv_row_warp(const CG& A, const Grp<kRowG>& q
     if (k < L) acc0 += __ldcs(a + k) * (double)v[__ldcs(c + k)];
     double acc = q.sum(acc0 + acc1);
     return A.diag[i] * (double)v[i] + acc;
+}
+
+template <typename V>
+__device__ __forceinline__ double spmv_row_warp(const CG& A, const Grp<kRowG>& q,
+                                                const V* __restrict__ v, int i)
+{
+    return spmv_row(A, q, v, i, A.moff[i], A.mlen[i]);
 }
 
 // (A32 v)_i for the inner solve of the mixed-precision path: FP32 values,
@@ -353,11 +363,16 @@ __global__ void k_cg_spmv(CG A, const double* __restrict__ p, double* __restrict
     Grp<kRowG> q;
     const long nwarps = (long)gridDim.x * blockDim.x / kRowG;
     double ps = 0;
+    // one 8-byte load of (offset, length) per row; length -1 marks rows
+    // outside the system (measured 0.569 against 0.574 ms per launch with
+    // bcon, mlen and moff read separately; prefetching the next row's pair
+    // costs 0.64 ms)
     for (long w = q.gid; w < A.n; w += nwarps) {
         int i = (int)w;
+        const int2 m = A.mrow[i];
         double si = 0;
-        if (A.bcon[i] == 0) {
-            si = spmv_row_warp(A, q, p, i);
+        if (m.y >= 0) {
+            si = spmv_row(A, q, p, i, m.x, m.y);
             if (q.lane == 0) ps += p[i] * si;
         }
         if (q.lane == 0) s[i] = si;
@@ -770,7 +785,7 @@ int vmps_ppe_apply(mps_ctx* c, const double* x, double* y)
 {
     int sms = 0;
     VMPS_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-    CG G{c->mcol, c->mval, c->mlen, c->moff, c->diag, c->bcon, c->cap_l, c->n, 0, 0, 0};
+    CG G{c->mcol, c->mval, c->mlen, c->moff, c->diag, c->bcon, c->cap_l, c->n, 0, 0, 0, c->mrow};
     k_apply<<<sms * 8, kRedThreads, 0, c->stream>>>(G, x, y);
     vmps_count_launch(1);
     VMPS_CUDA(c, cudaGetLastError());
@@ -818,12 +833,12 @@ int vmps_ppe(mps_ctx* c)
         k_assemble<3><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
                                                   nsrc, warm, c->pnew, c->pold, c->moff, c->mcol,
                                                   c->mval, c->mcv32, c->mlen, c->diag, c->source,
-                                                  w_bcon);
+                                                  w_bcon, c->mrow);
     else
         k_assemble<2><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
                                                   nsrc, warm, c->pnew, c->pold, c->moff, c->mcol,
                                                   c->mval, c->mcv32, c->mlen, c->diag, c->source,
-                                                  w_bcon);
+                                                  w_bcon, c->mrow);
     vmps_count_launch(1);
     if (f.srcopt) {
         // slot of particle id k: inv_id[k] (the sort's inv buffer is free here)
@@ -853,7 +868,7 @@ int vmps_ppe(mps_ctx* c)
     // zero initial guess (the assembly zeroed pnew): r = b exactly, so the
     // start kernels skip the product A x0
     CG G{c->mcol, c->mval, c->mlen, c->moff, c->diag, c->bcon, c->cap_l, n,
-         f.solver == 1 ? 1 : 0, nblk, warm == 0 ? 1 : 0};
+         f.solver == 1 ? 1 : 0, nblk, warm == 0 ? 1 : 0, c->mrow};
     double tol2 = f.cg_tol * f.cg_tol;
     const bool batched = c->nscenes > 1;
     // Inside a stream capture (graph mode) the loop becomes a conditional
