@@ -266,10 +266,9 @@ __device__ __forceinline__ double spmv_row_warp(const CG& A, const Grp<kRowG>& q
 // entry), and each lane keeps four entries in flight.
 __device__ __forceinline__ float spmv_row_warp32(const CG& A, const int2* __restrict__ cv,
                                                  const Grp<kRowG>& q, const float* __restrict__ v,
-                                                 int i)
+                                                 int i, int off, int L)
 {
-    const int L = A.mlen[i];
-    const int2* __restrict__ e = cv + A.moff[i];
+    const int2* __restrict__ e = cv + off;
     float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc3 = 0.f;
     int k = q.lane;
     for (; k + 3 * kRowG < L; k += 4 * kRowG) {
@@ -636,18 +635,19 @@ __global__ void k_ir_spmv(CG A, IR I, double* __restrict__ r64, double* __restri
     double acc = 0;
     for (long w = q.gid; w < A.n; w += nwarps) {
         int i = (int)w;
-        if (A.bcon[i] != 0) {
+        const int2 m = A.mrow[i];  // (offset, length); length -1: outside the system
+        if (m.y < 0) {
             if (phase == 0 && q.lane == 0) I.s[i] = 0.f;
             continue;
         }
         if (phase == 0) {
-            float si = spmv_row_warp32(A, I.cv, q, I.p, i);
+            float si = spmv_row_warp32(A, I.cv, q, I.p, i, m.x, m.y);
             if (q.lane == 0) {
                 I.s[i] = si;
                 acc += (double)I.p[i] * (double)si;
             }
         } else {
-            double t = spmv_row_warp(A, q, I.d, i);
+            double t = spmv_row(A, q, I.d, i, m.x, m.y);
             if (q.lane == 0) {
                 double ri = r64[i] - t;
                 r64[i] = ri;
