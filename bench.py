@@ -10,8 +10,9 @@ collision, commit).  ``value`` is whole-job particle-steps/s with the state
 resident in HBM; ``e2e`` is the same metric through the public API with host
 buffers (state uploaded from pinned host memory and downloaded every step).
 Under torchrun each rank advances its own copy of the scene (independent
-scenes, no collective on the data path: weak scaling); timings are the max
-over ranks.  ``--impl reference`` times the reference's own CPU path
+scenes, no collective on the data path: weak scaling), except that the
+batched configuration (--config 4) splits its 64 scenes between the ranks
+(strong scaling, still no exchange); timings are the max over ranks.  ``--impl reference`` times the reference's own CPU path
 (oracle/_ref, OpenMP on all host cores) on a bounded sample of the workload.
 """
 from __future__ import annotations
@@ -55,6 +56,17 @@ def max_over_ranks(v: float, ws: int, device: str = "cuda") -> float:
     import torch.distributed as dist
     t = torch.tensor([v], device=device, dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(v: float, ws: int, device: str = "cuda") -> float:
+    """Sum of a per-rank count over all ranks (every rank gets it)."""
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
 
@@ -163,15 +175,21 @@ WORKLOADS = {
 }
 
 
-def build_case(scale: int = 0, which: int = 1, precision=None):
+def build_case(scale: int = 0, which: int = 1, precision=None, rank: int = 0, ws: int = 1):
     """(cfg, case, scenes) of the benchmark scene; scale > 0 selects the
-    smaller 3D dam used for profiling captures (config.scaled_dam3d)."""
+    smaller 3D dam used for profiling captures (config.scaled_dam3d).  The
+    batched configuration's independent scenes are split over the ws ranks
+    (config.partition_scenes); every other configuration is one scene, which
+    each rank advances as its own replica."""
     from voxarmps_b200 import config
     scenes = None
     if scale:
         cfg, case = config.scaled_dam3d(scale)
     elif which == 4:
         base, sc = config.baseline(4)
+        if ws > 1:
+            part = config.partition_scenes([len(s["x"]) for s in sc], ws)[rank]
+            sc = [sc[k] for k in part]
         cfg, case, sid, boxes, pmax = config.batched(base, sc)
         scenes = (sid, boxes, pmax)
     else:
@@ -254,7 +272,8 @@ def run_ours(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    cfg, case, scenes = build_case(args.scale, args.config, args.precision)
+    cfg, case, scenes = build_case(args.scale, args.config, args.precision, rank, ws)
+    split = scenes is not None and ws > 1  # the batch's scenes are shared out
     mixed = cfg["precision"] == 1
     n = len(case["x"])
     fp = int((case["ptype"] > 0).sum())
@@ -372,20 +391,29 @@ def run_ours(args):
     if rank == 0:
         cpu = (time_reference(steps=3, warmup=1, nthreads=os.cpu_count() or 1)
                if ws == 1 and args.config in (1, 2) and not args.scale else None)
-        value = whole_job_rate(n * args.steps, ws, el_ms)
+    # units of the whole job: a split batch counts every rank's own particles
+    n_job = sum_over_ranks(float(n), ws) if split else float(n) * ws
+    fp_job = sum_over_ranks(float(fp), ws) if split else float(fp) * ws
+    if rank == 0:
+        value = whole_job_rate(n_job * args.steps, 1, el_ms)
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": el_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64",
+            "scaling": "strong" if split else "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if mixed else "f64",
             "data": "synthetic",
             "config": {"workload": (WORKLOADS[args.config] if not args.scale else
                                     f"3D dam break scaled x{args.scale} (profiling case)"),
-                       "particles": n, "fluid_particles": fp,
-                       "parallelism": (f"{ws} independent replicas" if ws > 1 else "1 GPU") +
-                                      (f", {int(scenes[2].shape[0])} scenes in one context"
-                                       if scenes is not None else ""),
+                       "particles": int(n_job) if split else n,
+                       "fluid_particles": int(fp_job) if split else fp,
+                       "parallelism": ((f"{ws} ranks, the batch's scenes split between them "
+                                        f"(rank 0: {int(scenes[2].shape[0])} scenes, {n} "
+                                        "particles, in one context), no exchange") if split else
+                                       (f"{ws} independent replicas" if ws > 1 else "1 GPU") +
+                                       (f", {int(scenes[2].shape[0])} scenes in one context"
+                                        if scenes is not None else "")),
                        "l2": "working set (lists, matrix) > 126 MB L2; no flush needed"},
-            "fluid_particle_steps_per_s": fp * args.steps * ws / (el_ms * 1e-3),
+            "fluid_particle_steps_per_s": fp_job * args.steps / (el_ms * 1e-3),
             "graph": bool(args.graph), "ms_per_step_profiled_eager": prof_ms / args.steps,
             "tuning": dict(tuning, autotuned=bool(args.autotune)),
             "ppe_ms_per_step": statistics.mean(ppe_ms), "cg_iters_mean": statistics.mean(iters),
@@ -404,7 +432,7 @@ def run_ours(args):
                          "avg_launch_ms": spmv_avg_ms, "launches_timed": int(spmv_n),
                          "duration_source": "CUDA events around every %s launch over the "
                                             "K profiled steps" % ("k_ir_spmv" if mixed else "k_cg_spmv")},
-            "e2e": {"value": whole_job_rate(n * args.steps, ws, e2e_ms), "unit": METRIC,
+            "e2e": {"value": whole_job_rate(n_job * args.steps, 1, e2e_ms), "unit": METRIC,
                     "h2d_bytes_per_step": bytes_state, "d2h_bytes_per_step": bytes_state},
             "gpu_launches": launches, "clocks": clocks,
             "cpu_baseline": ({k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}

@@ -122,6 +122,23 @@ def baseline(idx: int):
     return with_box(cfg, case), case
 
 
+def partition_scenes(sizes, ws: int):
+    """Split independent scenes over ws ranks by particle count (largest
+    first, each to the least-loaded rank; ties to the lower rank): a list of
+    ws lists of scene indices, each in increasing order.  Deterministic, so
+    every rank computes the same split without exchanging anything."""
+    if ws < 1:
+        raise ValueError("ws must be >= 1")
+    load = [0] * ws
+    parts = [[] for _ in range(ws)]
+    order = sorted(range(len(sizes)), key=lambda k: (-int(sizes[k]), k))
+    for k in order:
+        r = min(range(ws), key=lambda q: (load[q], q))
+        parts[r].append(k)
+        load[r] += int(sizes[k])
+    return [sorted(p) for p in parts]
+
+
 def batched(cfg: dict, scenes, gap_radii: float = 4.0):
     """(cfg, stacked case, scene ids, boxes, pmax) for scenes advanced in one
     context; the gap between scenes is gap_radii Laplacian radii."""
