@@ -579,24 +579,36 @@ static int enqueue_step(mps_ctx* c)
         return MPS_OK;
     };
     TRY(mark(0));
-    if (f.method != 3 && !f.ppe_at_predicted) TRY(vmps_pnd(c, 0, 1, 1, c->nd));
-    TRY(vmps_neighbors(c));
+    {
+        NvtxRange r("mps.neighbors");
+        if (f.method != 3 && !f.ppe_at_predicted) TRY(vmps_pnd(c, 0, 1, 1, c->nd));
+        TRY(vmps_neighbors(c));
+    }
     TRY(mark(1));
-    if (f.turb) TRY(vmps_sps(c));
-    TRY(vmps_vfraction(c));
-    TRY(vmps_viscosity(c));
-    TRY(vmps_predict(c));
-    TRY(vmps_pnd(c, 1, 0, 1, c->nds));
-    if (f.method != 3) TRY(vmps_bcon(c));
+    {
+        NvtxRange r("mps.explicit");
+        if (f.turb) TRY(vmps_sps(c));
+        TRY(vmps_vfraction(c));
+        TRY(vmps_viscosity(c));
+        TRY(vmps_predict(c));
+        TRY(vmps_pnd(c, 1, 0, 1, c->nds));
+        if (f.method != 3) TRY(vmps_bcon(c));
+    }
     TRY(mark(2));
-    if (f.method != 3) TRY(vmps_ppe(c));
-    else TRY(vmps_pressure_wc(c));
+    {
+        NvtxRange r("mps.pressure");
+        if (f.method != 3) TRY(vmps_ppe(c));
+        else TRY(vmps_pressure_wc(c));
+    }
     TRY(mark(3));
-    TRY(vmps_phat(c));
-    TRY(vmps_pressgrad(c));
-    TRY(vmps_integrate(c));
-    TRY(vmps_collision(c));
-    TRY(vmps_commit(c));
+    {
+        NvtxRange r("mps.post");
+        TRY(vmps_phat(c));
+        TRY(vmps_pressgrad(c));
+        TRY(vmps_integrate(c));
+        TRY(vmps_collision(c));
+        TRY(vmps_commit(c));
+    }
     TRY(mark(4));
     return MPS_OK;
 }
@@ -610,6 +622,7 @@ static int graph_step(mps_ctx* c)
     if (!c->stream2) VMPS_CUDA(c, cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
     TRY(vmps_gnn_prepare(c));  // no allocation inside the capture
     if (!c->gexec[par]) {
+        NvtxRange nr("mps.graph_capture");
         const long long l0 = g_launches.load();
         VMPS_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
         int r = enqueue_step(c);
@@ -639,6 +652,7 @@ static int graph_step(mps_ctx* c)
 int mps_step(mps_ctx* c)
 {
     NEED_INIT(c);
+    NvtxRange nr("mps.step");
     VMPS_CUDA(c, cudaSetDevice(c->device));
     unsigned int before = c->host_err;
     const bool graph = c->use_graph && !c->profile;
@@ -1006,6 +1020,7 @@ struct Fnv {
 
 int mps_save_checkpoint(mps_ctx* c, const char* path)
 {
+    NvtxRange nr("mps.save_checkpoint");
     NEED_INIT(c);
     if (!path) return MPS_ERR_ARG;
     const int n = c->n, ns = c->nscenes;
@@ -1063,6 +1078,7 @@ int mps_save_checkpoint(mps_ctx* c, const char* path)
 
 int mps_load_checkpoint(mps_ctx* c, const char* path)
 {
+    NvtxRange nr("mps.load_checkpoint");
     if (!c || !path) return MPS_ERR_ARG;
     FILE* fp = fopen(path, "rb");
     if (!fp) {
@@ -1214,6 +1230,7 @@ static int write_vtu_binary(const char* path, int n, const double* s, bool three
 
 int mps_snapshot_vtu(mps_ctx* c, const char* path, int fluid_only)
 {
+    NvtxRange nr("mps.snapshot_vtu");
     NEED_INIT(c);
     if (!path) return MPS_ERR_ARG;
     snap_join(c);  // one snapshot in flight: its buffers are reused

@@ -11,6 +11,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -20,6 +21,15 @@
 #include <vector>
 
 #include "../../include/voxarmps.h"
+
+// NVTX range over a host scope (stages, graph capture and replay, I/O): a
+// profiler's timeline shows them; without one attached they cost nothing
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 namespace vmps {
 
