@@ -79,3 +79,17 @@ def test_invalid_config_rejected_without_gpu(lib):
     c = vm.MpsConfig(**{k: cfg[k] for k, _ in config.FIELDS})
     h = C.c_void_p()
     assert lib.mps_create(C.byref(c), 0, C.byref(h)) == vm.MPS_ERR_ARG
+
+
+def test_status_codes_match_header():
+    """Every MPS_OK / MPS_ERR_* bit the header defines has the same value in
+    the Python layer, and the bits are distinct powers of two."""
+    text = open(HEADER).read()
+    codes = {k: int(v) for k, v in re.findall(r"#define\s+(MPS_(?:OK|ERR_\w+))\s+(\d+)", text)}
+    assert codes["MPS_OK"] == 0 and len(codes) >= 9
+    for name, value in codes.items():
+        assert getattr(vm, name) == value, name
+    bits = [v for k, v in codes.items() if k != "MPS_OK"]
+    assert len(set(bits)) == len(bits)
+    assert all(b > 0 and b & (b - 1) == 0 for b in bits)
+    assert vm.FATAL == codes["MPS_ERR_ARG"] | codes["MPS_ERR_CUDA"] | codes["MPS_ERR_IO"]
