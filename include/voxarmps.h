@@ -148,6 +148,12 @@ int mps_set_state(mps_ctx* ctx, const double* x, const double* y, const double* 
                   const double* u, const double* v, const double* w, const double* p);
 int mps_get_state(mps_ctx* ctx, double* x, double* y, double* z, double* u, double* v,
                   double* w, double* p);
+/* Overwrite one state array between stage calls, host doubles in the caller's
+ * particle order: x y z u v w (the packed copies the stages read follow),
+ * p, pnew, un vn wn (the corrected velocity COLLISION2 and PREPDATA read).
+ * The reference's caller owns these arrays and may write them between any
+ * two calls of main.cu's loop (main.cu:1027-1363); this is that write. */
+int mps_set_field(mps_ctx* ctx, const char* field, const double* in);
 /* Per-stage device timing with CUDA events (off by default).  While on,
  * scalars ms_neighbors ms_explicit ms_ppe ms_post ms_step (last step) and
  * spmv_ms / spmv_launches, lists_ms (accumulated) are available. */
@@ -241,9 +247,11 @@ void* mps_stream(mps_ctx* ctx);
  * set non-zero when a particle lies outside the grid; stream: cudaStream_t
  * or NULL.  Limits: n <= 262,144 particles and at most 262,142 cells;
  * larger inputs return MPS_ERR_ARG.  Scratch is a fixed static device area
- * shared by all calls (calls that overlap on the GPU race); the first call
- * on each device looks its address up and should come before any stream
- * capture.  Asynchronous on stream. */
+ * shared by all calls (calls that overlap on the GPU race); a call outside
+ * a stream capture looks its address up (again after a cudaDeviceReset), a
+ * call during a capture reuses the last address found on that device, so
+ * the first call on each device should come before any stream capture.
+ * Asynchronous on stream. */
 int mps_cell_order_noalloc(const mps_config* cfg, double re, int n, const double* x,
                            const double* y, const double* z, int* cell, int* perm,
                            unsigned int* out_of_grid, void* stream);

@@ -868,55 +868,100 @@ void mo_collision(const mo_params* P, int n, const int* off, const int* nbr, con
     }
 }
 
-/* Order-independent collision: every colliding pair (d < coll, approaching)
-   exchanges the same impulse COLLISION2 applies, evaluated from the
-   pre-collision state and gathered by each particle from its own list.  The
-   pair impulse is symmetric (vabs_ij == vabs_ji), so for pairs that do not
-   share a particle the result equals COLLISION2's. */
+/* One visit of COLLISION2's pair loop (functions.cu:1536-1599) from particle
+   i's list to its neighbour j, on local copies of their states
+   s = {u, v, w, x, y, z}: the same expressions, in the same order, as the
+   reference's in-place update of unew/vnew/wnew and x/y/z. */
+static void coll_visit(const mo_params* P, int dim, int pti, int ptj, double* si, double* sj)
+{
+    double m1 = (pti == 1) ? P->rho1 : P->rho2;
+    double m2 = (ptj == 1) ? P->rho1 : P->rho2;
+    double DT = P->dt, cc = P->cc;
+    double dx = sj[3] - si[3], dy = sj[4] - si[4], dz = 0, d;
+    if (dim == 3) {
+        dz = sj[5] - si[5];
+        d = sqrt(dx * dx + dy * dy + dz * dz);
+    } else {
+        d = sqrt(dx * dx + dy * dy);
+    }
+    if (!(d < P->coll)) return;
+    double ug = (m1 * si[0] + m2 * sj[0]) / (m1 + m2);
+    double vg = (m1 * si[1] + m2 * sj[1]) / (m1 + m2);
+    double wg = 0, wr = 0, wm = 0, vabs;
+    if (dim == 3) wg = (m1 * si[2] + m2 * sj[2]) / (m1 + m2);
+    double ur = m1 * (si[0] - ug);
+    double vr = m1 * (si[1] - vg);
+    if (dim == 3) wr = m1 * (si[2] - wg);
+    if (dim == 3)
+        vabs = (ur * dx + vr * dy + wr * dz) / d;
+    else
+        vabs = (ur * dx + vr * dy) / d;
+    double um = (1.0 + cc) * vabs * dx / d;
+    double vm = (1.0 + cc) * vabs * dy / d;
+    if (dim == 3) wm = (1.0 + cc) * vabs * dz / d;
+    if (!(vabs > 0)) return;
+    if (pti > 0) {
+        si[0] = si[0] - um / m1; si[1] = si[1] - vm / m1;
+        si[3] = si[3] - DT * um / m1; si[4] = si[4] - DT * vm / m1;
+        if (dim == 3) { si[2] = si[2] - wm / m1; si[5] = si[5] - DT * wm / m1; }
+    }
+    if (ptj > 0) {
+        sj[0] = sj[0] + um / m2; sj[1] = sj[1] + vm / m2;
+        sj[3] = sj[3] + DT * um / m2; sj[4] = sj[4] + DT * vm / m2;
+        if (dim == 3) { sj[2] = sj[2] + wm / m2; sj[5] = sj[5] + DT * wm / m2; }
+    }
+}
+
+/* Order-independent collision.  COLLISION2 walks every particle (walls and
+   dummies included) in id order and updates pairs in place, so a pair
+   (a, b), a < b, is visited twice: from a's list, then from b's list with
+   the state the first visit left.  A fluid-fluid pair's second visit finds
+   the pair separating and does nothing; a fluid-wall pair can be pushed
+   again, because the wall keeps its velocity.  Here every fluid particle
+   replays, for each neighbour closer than coll in the pre-collision state,
+   that pair's two visits on private copies.  With one such neighbour the
+   particle takes the replayed state itself -- bit for bit COLLISION2's,
+   since nothing else touches the pair in between; with several it takes
+   the pre-collision state plus the sum of the pairs' changes, in list
+   order, where the sequential result would depend on the visiting order. */
 void mo_collision_gather(const mo_params* P, int n, const int* off, const int* nbr,
                          const int* ptype, double* un, double* vn, double* wn, double* x,
                          double* y, double* z)
 {
     int dim = P->dim;
-    double DT = P->dt, cc = P->cc;
-    size_t sz = sizeof(double) * (size_t)(n > 0 ? n : 1);
-    double *du = (double*)calloc(1, sz), *dv = (double*)calloc(1, sz), *dw = (double*)calloc(1, sz);
-    double *dx = (double*)calloc(1, sz), *dy = (double*)calloc(1, sz), *dz = (double*)calloc(1, sz);
+    size_t sz = sizeof(double) * 6 * (size_t)(n > 0 ? n : 1);
+    double* out = (double*)malloc(sz);
     for (int i = 0; i < n; i++) {
+        double s0[6] = {un[i], vn[i], dim == 3 ? wn[i] : 0.0, x[i], y[i], dim == 3 ? z[i] : 0.0};
+        double acc[6] = {0, 0, 0, 0, 0, 0}, last[6];
+        int hits = 0;
+        for (int k = 0; k < 6; k++) { out[6 * (size_t)i + k] = s0[k]; last[k] = s0[k]; }
         if (ptype[i] <= 0) continue;
-        double m1 = (ptype[i] == 1) ? P->rho1 : P->rho2;
         for (int l = off[i]; l < off[i + 1]; l++) {
             int j = nbr[l];
-            double d = dist(dim, i, j, x, y, z);
-            if (i == j || !(d < P->coll)) continue;
-            double m2 = (ptype[j] == 1) ? P->rho1 : P->rho2;
-            double ug = (m1 * un[i] + m2 * un[j]) / (m1 + m2);
-            double vg = (m1 * vn[i] + m2 * vn[j]) / (m1 + m2);
-            double wg = 0, wr = 0, vabs;
-            if (dim == 3) wg = (m1 * wn[i] + m2 * wn[j]) / (m1 + m2);
-            double ur = m1 * (un[i] - ug), vr = m1 * (vn[i] - vg);
-            if (dim == 3) wr = m1 * (wn[i] - wg);
-            if (dim == 3)
-                vabs = (ur * (x[j] - x[i]) + vr * (y[j] - y[i]) + wr * (z[j] - z[i])) / d;
-            else
-                vabs = (ur * (x[j] - x[i]) + vr * (y[j] - y[i])) / d;
-            if (!(vabs > 0)) continue;
-            double um = (1.0 + cc) * vabs * (x[j] - x[i]) / d;
-            double vm = (1.0 + cc) * vabs * (y[j] - y[i]) / d;
-            du[i] -= um / m1; dv[i] -= vm / m1;
-            dx[i] -= DT * um / m1; dy[i] -= DT * vm / m1;
-            if (dim == 3) {
-                double wm = (1.0 + cc) * vabs * (z[j] - z[i]) / d;
-                dw[i] -= wm / m1; dz[i] -= DT * wm / m1;
+            if (j == i || !(dist(dim, i, j, x, y, z) < P->coll)) continue;
+            double si[6] = {s0[0], s0[1], s0[2], s0[3], s0[4], s0[5]};
+            double sj[6] = {un[j], vn[j], dim == 3 ? wn[j] : 0.0, x[j], y[j],
+                            dim == 3 ? z[j] : 0.0};
+            if (j < i) {
+                coll_visit(P, dim, ptype[j], ptype[i], sj, si);
+                coll_visit(P, dim, ptype[i], ptype[j], si, sj);
+            } else {
+                coll_visit(P, dim, ptype[i], ptype[j], si, sj);
+                coll_visit(P, dim, ptype[j], ptype[i], sj, si);
             }
+            for (int k = 0; k < 6; k++) { acc[k] += si[k] - s0[k]; last[k] = si[k]; }
+            hits++;
         }
+        for (int k = 0; k < 6; k++)
+            out[6 * (size_t)i + k] = hits == 1 ? last[k] : (hits > 1 ? s0[k] + acc[k] : s0[k]);
     }
     for (int i = 0; i < n; i++) {
-        if (ptype[i] <= 0) continue;
-        un[i] += du[i]; vn[i] += dv[i]; x[i] += dx[i]; y[i] += dy[i];
-        if (dim == 3) { wn[i] += dw[i]; z[i] += dz[i]; }
+        const double* o = out + 6 * (size_t)i;
+        un[i] = o[0]; vn[i] = o[1]; x[i] = o[3]; y[i] = o[4];
+        if (dim == 3) { wn[i] = o[2]; z[i] = o[5]; }
     }
-    free(du); free(dv); free(dw); free(dx); free(dy); free(dz);
+    free(out);
 }
 
 /* EULERINTEGRATION + BOUNDARIE (dam test), functions.cu:1963-2021 */

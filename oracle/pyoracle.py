@@ -22,6 +22,17 @@ LIB_ORACLE = os.path.join(HERE, "liboracle.so")
 LIB_REF = os.path.join(HERE, "_ref", "libref.so")
 LIB_REF_OMP = os.path.join(HERE, "_ref", "libref_omp.so")
 
+# Where the reference's sources lie: the environment variable
+# VOXARMPS_REFERENCE, by default /root/reference.  Only the recipes that
+# compile the reference (oracle/Makefile) and the scripts that read its
+# inputs (tests/golden/make_golden.py, the generator parity test) use it.
+REFERENCE_ROOT = os.environ.get("VOXARMPS_REFERENCE", "/root/reference")
+
+
+def reference_path(*parts: str) -> str:
+    """A path under the reference's source tree."""
+    return os.path.join(REFERENCE_ROOT, *parts)
+
 
 class MoParams(C.Structure):
     """Mirror of ``mo_params`` in mps_oracle.h (field order matters)."""
@@ -50,7 +61,8 @@ class MoParams(C.Structure):
 def build(ref: bool = False) -> None:
     """Compile liboracle.so (and the reference libraries when ``ref``)."""
     targets = ["all"] + (["ref"] if ref else [])
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"REFERENCE={REFERENCE_ROOT}"] + targets,
+                   check=True)
 
 
 def params_from(cfg: dict) -> MoParams:
@@ -107,6 +119,9 @@ def _load_oracle():
                               _IP, _IP, _DP, _DP, _DP, _IP, _DP, _DP]
     lib.mo_lambda.restype = C.c_double
     lib.mo_lambda.argtypes = [C.c_int, C.c_double]
+    for name in ("mo_collision", "mo_collision_gather"):
+        getattr(lib, name).argtypes = [C.POINTER(MoParams), C.c_int, _IP, _IP, _IP, _DP, _DP,
+                                       _DP, _DP, _DP, _DP]
     return lib
 
 
@@ -193,6 +208,9 @@ def _load_ref(omp: bool):
         lib.rh_scalar.restype = C.c_double
         lib.rh_scalar.argtypes = [C.c_void_p, C.c_char_p]
         lib.rh_destroy.argtypes = [C.c_void_p]
+        lib.rh_set.restype = C.c_long
+        lib.rh_set.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p]
+        lib.rh_stage.argtypes = [C.c_void_p, C.c_char_p]
         _REF[path] = lib
     return _REF[path]
 
@@ -225,12 +243,36 @@ class RefHarness(_StateBase):
     def scalar(self, name):
         return self.lib.rh_scalar(self.h, name.encode())
 
+    def set(self, name, arr):
+        arr = np.ascontiguousarray(arr, dtype=np.float64)
+        if self.lib.rh_set(self.h, name.encode(), arr.ctypes.data_as(C.c_void_p)) < 0:
+            raise KeyError(name)
+
+    def stage(self, name):
+        """One reference routine by its name ("NEIGHBOR", "COLLISION2")."""
+        if self.lib.rh_stage(self.h, name.encode()) != 0:
+            raise KeyError(name)
+
     def close(self):
         if self.h:
             self.lib.rh_destroy(self.h)
             self.h = None
 
     __del__ = close
+
+
+def collision(cfg: dict, off, nbr, ptype, un, vn, wn, x, y, z, gather: bool = False):
+    """COLLISION2 on copies of the inputs: the sequential in-place form
+    (mo_collision) or the order-independent gather (mo_collision_gather).
+    Returns (un, vn, wn, x, y, z)."""
+    lib = oracle_lib()
+    P = params_from(cfg)
+    a = [np.array(v, np.float64) for v in (un, vn, wn, x, y, z)]
+    fn = lib.mo_collision_gather if gather else lib.mo_collision
+    fn(C.byref(P), len(a[0]), _ip(np.ascontiguousarray(off, np.int32)),
+       _ip(np.ascontiguousarray(nbr, np.int32)), _ip(np.ascontiguousarray(ptype, np.int32)),
+       *[_dp(v) for v in a])
+    return tuple(a)
 
 
 def W(r, ktype, dim, re):

@@ -221,6 +221,43 @@ long rh_get(void* h, const char* name, void* out)
     return -1;
 }
 
+/* Overwrite one double field (0-based input) between stage calls, as
+   main.cu's caller-owned arrays allow.  Returns the count or -1. */
+long rh_set(void* h, const char* name, const void* in)
+{
+    RefState* S = (RefState*)h;
+    struct { const char* nm; double* a; } dbl[] = {
+        {"x", S->x}, {"y", S->y}, {"z", S->z}, {"u", S->u}, {"v", S->v}, {"w", S->w},
+        {"p", S->p}, {"pnew", S->pnew}, {"un", S->unew}, {"vn", S->vnew}, {"wn", S->wnew}};
+    for (auto& d : dbl)
+        if (!strcmp(name, d.nm)) {
+            memcpy(d.a + 1, in, sizeof(double) * (size_t)S->TP);
+            return S->TP;
+        }
+    return -1;
+}
+
+/* One reference routine on the harness state: "NEIGHBOR" (at re_s, the
+   harness radius) or "COLLISION2" (functions.cu:2788, 1523), called with
+   main.cu's arguments.  Returns 0, or -1 for an unknown name. */
+int rh_stage(void* h, const char* name)
+{
+    RefState* S = (RefState*)h;
+    const mo_params& P = S->P;
+    omp_set_num_threads(S->nthreads);
+    if (!strcmp(name, "NEIGHBOR")) {
+        NEIGHBOR(P.xmax, P.xmin, P.ymax, P.ymin, P.zmax, P.zmin, P.re_s, P.delta, S->TP, S->x,
+                 S->y, S->z, S->neighb, S->DIM, S->codeOpt);
+        return 0;
+    }
+    if (!strcmp(name, "COLLISION2")) {
+        COLLISION2(S->TP, P.coll, S->PTYPE, P.rho1, P.rho2, S->neighb, P.cc, S->unew, S->vnew,
+                   S->wnew, S->x, S->y, S->z, P.dt, S->DIM, S->codeOpt);
+        return 0;
+    }
+    return -1;
+}
+
 /* the reference's kernel function itself (functions.cu:32-74) */
 double rh_W(double r, int ktype, int dim, double re) { return W(r, ktype, dim, re); }
 

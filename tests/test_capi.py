@@ -93,3 +93,15 @@ def test_status_codes_match_header():
     assert len(set(bits)) == len(bits)
     assert all(b > 0 and b & (b - 1) == 0 for b in bits)
     assert vm.FATAL == codes["MPS_ERR_ARG"] | codes["MPS_ERR_CUDA"] | codes["MPS_ERR_IO"]
+
+
+def test_cpp_driver_compiles_and_links(tmp_path):
+    """tests/cpp/main_loop.cpp (the reference's loop in C++ against the
+    header) compiles and links against the library; it runs in
+    tests/test_gpu_cpp.py."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.join(root, "voxarmps_b200")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I",
+                    os.path.join(root, "include"), os.path.join(root, "tests", "cpp", "main_loop.cpp"),
+                    "-L", libdir, "-lvoxarmps_b200", "-o", str(tmp_path / "main_loop")], check=True)

@@ -9,18 +9,20 @@ import subprocess
 import numpy as np
 import pytest
 
+import pyoracle
 from voxarmps_b200 import gen
 
 ORACLE = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle")
 GEN_EXE = os.path.join(ORACLE, "_ref", "gen")
-REF_SRC = "/root/reference/generateSimulationCases/generateSimulationCases"
+REF_SRC = pyoracle.reference_path("generateSimulationCases", "generateSimulationCases")
 
 
 @pytest.fixture(scope="module")
 def ref_gen():
     if not os.path.isdir(REF_SRC):
         pytest.skip("reference generator sources not present")
-    subprocess.run(["make", "-s", "-C", ORACLE, "gen"], check=True)
+    subprocess.run(["make", "-s", "-C", ORACLE, f"REFERENCE={pyoracle.REFERENCE_ROOT}", "gen"],
+                   check=True)
     return GEN_EXE
 
 

@@ -1,0 +1,66 @@
+"""Cell numbers, sort permutations and both neighbour lists bit-exact against
+the oracle's NEIGHBOR (functions.cu:2788-2929, pinned to the reference by
+tests/test_oracle_pin.py) at the benchmark sizes (needs a B200):
+
+* the 3D dam break of the headline workload, 1,595,308 particles;
+* the two-phase scene, 86,118 particles;
+* the 64 batched dam breaks in one context, 345 k particles;
+
+each at the initial lattice and again after 20 GPU steps, when particles
+have left the lattice: the lists are rebuilt at the GPU's own positions
+(mps_neighbors) and the oracle bins the same positions.
+"""
+import numpy as np
+import pytest
+
+import pyoracle
+import voxarmps_b200 as vm
+from voxarmps_b200 import config
+from gpu_util import gpu_cfg
+
+pytestmark = pytest.mark.gpu
+
+
+def check_lists(g, cfg, what):
+    x, y, z = g.get("x"), g.get("y"), g.get("z")
+    for which, sfx, re in ((0, "s", cfg["re_s"]), (1, "l", cfg["re_l"])):
+        cell, perm, off, nbr = pyoracle.neighbor(cfg, re, x, y, z)
+        assert np.array_equal(g.get("cell_" + sfx), cell), f"{what}: cells {sfx}"
+        assert np.array_equal(g.get("perm_" + sfx), perm), f"{what}: permutation {sfx}"
+        goff, gnbr = g.lists(which)
+        assert np.array_equal(goff, off), f"{what}: list lengths {sfx}"
+        assert np.array_equal(gnbr, nbr), f"{what}: list entries {sfx}"
+        del cell, perm, off, nbr, goff, gnbr
+
+
+def run_case(cfg, case, scenes=None, steps=20):
+    g = vm.Solver(cfg, case)
+    if scenes is not None:
+        g.set_scenes(*scenes)
+    assert g.init() == 0
+    check_lists(g, cfg, "initial lattice")
+    g.set_graph(True)
+    for _ in range(steps):
+        assert g.step() == 0
+    # lists at the positions the 20 steps left
+    assert g.NEIGHBOR() == 0
+    assert np.abs(g.get("y") - np.asarray(case["y"])).max() > 0  # off the lattice
+    check_lists(g, cfg, f"after {steps} steps")
+    g.close()
+
+
+def test_dam3d_headline_size_lists_bit_exact():
+    cfg, case = config.baseline(1)
+    assert len(case["x"]) == 1595308
+    run_case(gpu_cfg(cfg), case)
+
+
+def test_two_phase_full_geometry_lists_bit_exact():
+    cfg, case = config.baseline(3)
+    run_case(gpu_cfg(cfg), case)
+
+
+def test_batched_64_scenes_lists_bit_exact():
+    base, scenes = config.baseline(4)
+    cfg, case, sid, boxes, pmax = config.batched(gpu_cfg(base, precision=1), scenes)
+    run_case(cfg, case, scenes=(sid, boxes, pmax))

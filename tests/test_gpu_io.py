@@ -75,6 +75,33 @@ def test_checkpoint_rejects_corruption(tmp_path):
     b.close()
 
 
+def _fnv1a64(data: bytes) -> int:
+    h = 14695981039346656037
+    for b in data:
+        h = ((h ^ b) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+def test_checkpoint_rejects_trailing_bytes(tmp_path):
+    """Extra bytes between the payload and the checksum are refused even when
+    the checksum is recomputed over them."""
+    cfg, case = config.baseline(0)
+    a = vm.Solver(gpu_cfg(cfg), case)
+    assert a.init() == 0
+    ck = tmp_path / "c.ck"
+    a.save_checkpoint(str(ck))
+    raw = open(ck, "rb").read()
+    payload = raw[:-8] + b"\0" * 16
+    assert _fnv1a64(raw[:-8]) == int.from_bytes(raw[-8:], "little")  # the format's checksum
+    open(ck, "wb").write(payload + _fnv1a64(payload).to_bytes(8, "little"))
+    b = vm.Solver(gpu_cfg(cfg))
+    with pytest.raises(vm.MpsError) as e:
+        b.load_checkpoint(str(ck))
+    assert e.value.code & vm.MPS_ERR_IO
+    a.close()
+    b.close()
+
+
 @pytest.mark.parametrize("which", ["dam2d", "dam3d"])
 def test_binary_snapshot_matches_state_and_ascii(tmp_path, which):
     cfg, case = config.baseline(0) if which == "dam2d" else config.scaled_dam3d(1)

@@ -13,7 +13,9 @@ import numpy as np
 import pytest
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-FILES = sorted(glob.glob(os.path.join(GOLDEN, "ref_*.npz")))
+# whole-step runs; the collision and .grd-input fixtures have their own tests
+FILES = sorted(f for f in glob.glob(os.path.join(GOLDEN, "ref_*.npz"))
+               if "snaps" in np.load(f).files)
 
 
 def _digest(off, nbr):

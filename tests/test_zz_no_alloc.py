@@ -70,3 +70,19 @@ def test_noalloc_rejects_sizes_beyond_its_limit():
                                    buf.data_ptr(), buf.data_ptr(), out.data_ptr(),
                                    out.data_ptr(), out.data_ptr(), None)
     assert r == vm.MPS_ERR_ARG
+
+
+def test_noalloc_rejects_grids_beyond_its_limit():
+    """A support radius so small that the cell count along each axis, and
+    their product, overflow 32 bits is refused before anything is launched."""
+    import torch
+    cfg, case = _scenes()[1]
+    lib = vm.load_library()
+    cs = _cfg_struct(cfg)
+    buf = torch.zeros(8, dtype=torch.float64, device="cuda")
+    out = torch.zeros(8, dtype=torch.int32, device="cuda")
+    for re in (1e-7, 1e-12):
+        r = lib.mps_cell_order_noalloc(C.byref(cs), re, 8, buf.data_ptr(), buf.data_ptr(),
+                                       buf.data_ptr(), out.data_ptr(), out.data_ptr(),
+                                       out.data_ptr(), None)
+        assert r == vm.MPS_ERR_ARG

@@ -43,7 +43,8 @@ EXPORTS = [
     "mps_pnd_star", "mps_bcon", "mps_pressure", "mps_phat", "mps_pressure_gradient",
     "mps_integrate", "mps_collision", "mps_commit", "mps_step", "mps_run", "mps_download",
     "mps_download_lists", "mps_get_scalar", "mps_get_error", "mps_last_message",
-    "mps_write_vtu", "mps_stream", "mps_set_state", "mps_get_state", "mps_set_profile",
+    "mps_write_vtu", "mps_stream", "mps_set_state", "mps_get_state", "mps_set_field",
+    "mps_set_profile",
     "mps_cell_order_noalloc", "mps_set_scenes", "mps_set_graph",
     "mps_gnn_create", "mps_gnn_use", "mps_gnn_train", "mps_gnn_params", "mps_gnn_features",
     "mps_gnn_forward", "mps_gnn_download", "mps_get_tuning", "mps_set_tuning", "mps_autotune",
@@ -96,6 +97,7 @@ def load_library(path: str = LIB_PATH):
     lib.mps_stream.restype = P
     lib.mps_set_state.argtypes = [P, P, P, P, P, P, P, P]
     lib.mps_get_state.argtypes = [P, P, P, P, P, P, P, P]
+    lib.mps_set_field.argtypes = [P, C.c_char_p, DP]
     lib.mps_set_profile.argtypes = [P, C.c_int]
     lib.mps_set_graph.argtypes = [P, C.c_int]
     FP = C.POINTER(C.c_float)
@@ -257,6 +259,13 @@ class Solver:
     def set_state(self, *ptrs):
         """Host pointers (ints) for x, y, z, u, v, w, p in caller order; 0 skips."""
         return self._chk(self.lib.mps_set_state(self.h, *[p or None for p in ptrs]), "set_state")
+
+    def set(self, name: str, values):
+        """Overwrite one state array (caller order) between stage calls."""
+        a = np.ascontiguousarray(values, np.float64)
+        if a.shape != (self.n,):
+            raise ValueError(f"{name}: expected {self.n} values")
+        return self._chk(self.lib.mps_set_field(self.h, name.encode(), _dp(a)), f"set {name}")
 
     def get_state(self, *ptrs):
         return self._chk(self.lib.mps_get_state(self.h, *[p or None for p in ptrs]), "get_state")

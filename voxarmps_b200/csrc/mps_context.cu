@@ -88,20 +88,13 @@ void free_all(mps_ctx* c)
     c->alts.clear();
 }
 
-// NEIGHBOR's grid (functions.cu:2790-2802)
-Grid make_grid(const mps_config& f, double re)
+// NEIGHBOR's grid (functions.cu:2790-2802); false when the box holds more
+// than 2^30 cells or is not a finite, non-inverted box
+constexpr long long kMaxCells = 1LL << 30;
+bool make_grid(const mps_config& f, double re, Grid* g)
 {
-    Grid g;
-    g.re = re;
-    g.rez = f.dim == 3 ? re + f.delta : re;
-    g.xmin = f.xmin;
-    g.ymin = f.ymin;
-    g.zmin = f.zmin;
-    g.ncx = (int)((f.xmax - f.xmin) / (re)) + 1;
-    g.ncy = (int)((f.ymax - f.ymin) / (re)) + 1;
-    g.ncz = f.dim == 3 ? (int)((f.zmax - f.zmin) / (re + f.delta)) + 1 : 1;
-    g.tnc = g.ncx * g.ncy * g.ncz;
-    return g;
+    return grid_for(f.xmin, f.xmax, f.ymin, f.ymax, f.zmin, f.zmax, f.dim, re, f.delta,
+                    kMaxCells, g);
 }
 
 int lattice_count(int dim, double ratio, bool inclusive)
@@ -385,10 +378,8 @@ int mps_upload(mps_ctx* c, int n, const double* x, const double* y, const double
         else { f.zmin = 99999999; f.zmax = -99999999; }
         f.pmax = (double)n * 4.50;
     }
-    c->gl = make_grid(f, f.re_l);
-    c->gs = make_grid(f, f.re_s);
-    if ((long long)c->gl.tnc > (1LL << 30) || (long long)c->gs.tnc > (1LL << 30)) {
-        c->msg = "cell grid too large";
+    if (!make_grid(f, f.re_l, &c->gl) || !make_grid(f, f.re_s, &c->gs)) {
+        c->msg = "cell grid too large (over 2^30 cells) or box not finite";
         return MPS_ERR_ARG;
     }
     // FP32 screening bound: coordinates stored relative to the box minimum
@@ -817,6 +808,32 @@ int mps_set_state(mps_ctx* c, const double* x, const double* y, const double* z,
     return MPS_OK;
 }
 
+int mps_set_field(mps_ctx* c, const char* field, const double* in)
+{
+    NEED_INIT(c);
+    if (!field || !in) return MPS_ERR_ARG;
+    static const char* const kSettable[] = {"x", "y", "z",    "u",  "v",  "w",
+                                            "p", "pnew", "un", "vn", "wn"};
+    std::string f(field);
+    bool ok = false;
+    for (const char* s : kSettable) ok = ok || f == s;
+    if (!ok || (c->cfg.dim == 2 && (f == "z" || f == "w" || f == "wn"))) {
+        c->msg = "mps_set_field: field " + f + " cannot be set";
+        return MPS_ERR_ARG;
+    }
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    const int n = c->n;
+    VMPS_CUDA(c, cudaMemcpyAsync(c->stage_in, in, sizeof(double) * n, cudaMemcpyHostToDevice,
+                                 c->stream));
+    k_permute_in<<<grid_blocks(n), kBlock, 0, c->stream>>>(n, c->oid, c->stage_in, field_d(c, f),
+                                                           nullptr);
+    vmps_count_launch(1);
+    // the packed copies the stages gather from follow the fields they pack
+    if (f == "x" || f == "y" || f == "z" || f == "u" || f == "v" || f == "w") TRY(vmps_pack(c));
+    VMPS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MPS_OK;
+}
+
 int mps_get_state(mps_ctx* c, double* x, double* y, double* z, double* u, double* v, double* w,
                   double* p)
 {
@@ -1136,6 +1153,8 @@ int mps_load_checkpoint(mps_ctx* c, const char* path)
         if (!get(boxes.data(), sizeof(double) * 6 * ns) || !get(pm.data(), sizeof(double) * ns))
             return bad("truncated scenes");
     }
+    // the payload must end exactly where the checksum starts
+    if (pos != all.size() - 8) return bad("trailing bytes before the checksum");
     c->cfg = cfg;
     TRY(mps_upload(c, n, d[0].data(), d[1].data(), d[2].data(), pt.data(), d[3].data(),
                    d[4].data(), d[5].data(), d[6].data()));

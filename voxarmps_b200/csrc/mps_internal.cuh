@@ -43,6 +43,39 @@ struct Grid {
     double xmin, ymin, zmin;
 };
 
+// NEIGHBOR's cell grid for support radius re over the box of f: each axis
+// count int((max - min) / size) + 1 (functions.cu:2790-2802).  The quotients
+// are checked in floating point before the conversion and the product is
+// formed in 64 bits, so a box that is not finite, inverted, or holds more
+// than max_cells cells (in total or along one axis) returns false instead of
+// wrapping around.
+inline bool grid_for(double xmin, double xmax, double ymin, double ymax, double zmin,
+                     double zmax, int dim, double re, double delta, long long max_cells,
+                     Grid* out)
+{
+    if (!(re > 0)) return false;
+    auto axis = [&](double lo, double hi, double size, int* n) {
+        const double q = (hi - lo) / size;
+        if (!(q >= 0.0) || !(q < (double)max_cells)) return false;  // NaN fails as well
+        *n = (int)q + 1;
+        return (long long)*n <= max_cells;
+    };
+    Grid g;
+    g.re = re;
+    g.rez = dim == 3 ? re + delta : re;
+    g.xmin = xmin;
+    g.ymin = ymin;
+    g.zmin = zmin;
+    g.ncz = 1;
+    if (!axis(xmin, xmax, re, &g.ncx) || !axis(ymin, ymax, re, &g.ncy)) return false;
+    if (dim == 3 && !axis(zmin, zmax, g.rez, &g.ncz)) return false;
+    const long long t = (long long)g.ncx * g.ncy * g.ncz;
+    if (t > max_cells) return false;
+    g.tnc = (int)t;
+    *out = g;
+    return true;
+}
+
 // Squared-distance thresholds equivalent to the reference's sqrt() compares
 // (sqrt is correctly rounded on host and device, so the equivalence is exact).
 struct Cutoff {

@@ -10,11 +10,14 @@
 // The scratch area is a file-scope __device__ array.  Every GPU that loads
 // this library holds it (kNoAllocScratchBytes, about 4 MiB) until the
 // process exits.  Host code cannot use the array's name as a device
-// address, so the first call on each device looks its address up with
-// cudaGetSymbolAddress while that device is current; make that first call
-// before any stream capture.  All calls share the one area and it keeps the
-// previous call's contents: the counters are cleared at the start of every
-// call, and calls that overlap on the GPU (two streams at once) race.
+// address, so every call made outside a stream capture looks the address up
+// with cudaGetSymbolAddress while the device is current (the module can be
+// reloaded at a new address after cudaDeviceReset) and keeps it per device;
+// a call made during a capture uses the kept address, so make the first call
+// on each device before any stream capture.  All calls share the one area
+// and it keeps the previous call's contents: the counters are cleared at
+// the start of every call, and calls that overlap on the GPU (two streams at
+// once) race.
 #include <mutex>
 
 #include "mps_internal.cuh"
@@ -100,18 +103,21 @@ __global__ void k_na_rank(int n, const int* __restrict__ cell, const NoAllocScra
     perm[b + r] = me;
 }
 
-// the device address of the scratch area, looked up once per device with
-// that device current
-int scratch_for_device(NoAllocScratch** out)
+// the device address of the scratch area on the current device: looked up
+// again outside a capture, the kept one during a capture
+int scratch_for_device(cudaStream_t st, NoAllocScratch** out)
 {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return MPS_ERR_CUDA;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) return MPS_ERR_CUDA;
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
+    if (cap == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MPS_ERR_CUDA;
         g_scratch_ptr[dev] = p;
     }
+    if (!g_scratch_ptr[dev]) return MPS_ERR_CUDA;  // first call inside a capture
     *out = (NoAllocScratch*)g_scratch_ptr[dev];
     return MPS_OK;
 }
@@ -126,23 +132,15 @@ extern "C" int mps_cell_order_noalloc(const mps_config* cfg, double re, int n, c
         (cfg->dim == 3 && !z) || (cfg->dim != 2 && cfg->dim != 3))
         return MPS_ERR_ARG;
     if (n > kNoAllocMaxParticles) return MPS_ERR_ARG;
+    // every axis count and the total are checked before they are multiplied
     Grid g;
-    g.re = re;
-    g.rez = cfg->dim == 3 ? re + cfg->delta : re;
-    g.xmin = cfg->xmin;
-    g.ymin = cfg->ymin;
-    g.zmin = cfg->zmin;
-    g.ncx = (int)((cfg->xmax - cfg->xmin) / (re)) + 1;
-    g.ncy = (int)((cfg->ymax - cfg->ymin) / (re)) + 1;
-    g.ncz = cfg->dim == 3 ? (int)((cfg->zmax - cfg->zmin) / (re + cfg->delta)) + 1 : 1;
-    if (g.ncx <= 0 || g.ncy <= 0 || g.ncz <= 0) return MPS_ERR_ARG;
-    long long tnc = (long long)g.ncx * g.ncy * g.ncz;
-    if (tnc + 2 > kNoAllocMaxCells) return MPS_ERR_ARG;
-    g.tnc = (int)tnc;
+    if (!grid_for(cfg->xmin, cfg->xmax, cfg->ymin, cfg->ymax, cfg->zmin, cfg->zmax, cfg->dim, re,
+                  cfg->delta, kNoAllocMaxCells - 2, &g))
+        return MPS_ERR_ARG;
     NoAllocScratch* S = nullptr;
-    int r = scratch_for_device(&S);
-    if (r != MPS_OK) return r;
     cudaStream_t st = (cudaStream_t)stream;
+    int r = scratch_for_device(st, &S);
+    if (r != MPS_OK) return r;
     const int m = g.tnc + 2;
     if (cudaMemsetAsync(S->cnt, 0, sizeof(int) * m, st) != cudaSuccess) return MPS_ERR_CUDA;
     if (cudaMemsetAsync(out_of_grid, 0, sizeof(unsigned int), st) != cudaSuccess)

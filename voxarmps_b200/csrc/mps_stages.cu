@@ -683,89 +683,147 @@ struct CollArgs {
     double coll2, cc, dt, rho1, rho2;
 };
 
-// COLLISION2 (functions.cu:1523-1601) in its order-independent form: each
-// fluid particle gathers the impulse of every approaching pair (d < coll)
-// from the pre-collision state.  The position and velocity changes go to the
-// delta arrays; k_collision_apply adds them once every particle has read the
+// One visit of COLLISION2's pair loop (functions.cu:1536-1599) from i's list
+// to its neighbour j, on register copies s = {u, v, w, x, y, z} of the two
+// states: the reference's expressions in the reference's order.
+template <int DIM>
+__device__ __forceinline__ void coll_visit(const CollArgs& A, int pti, int ptj, double* si,
+                                           double* sj)
+{
+    const double m1 = (pti == 1) ? A.rho1 : A.rho2, m2 = (ptj == 1) ? A.rho1 : A.rho2;
+    const double ex = sj[3] - si[3], ey = sj[4] - si[4], ez = DIM == 3 ? sj[5] - si[5] : 0.0;
+    const double d2 = dist2<DIM>(ex, ey, ez);
+    if (!(d2 < A.coll2)) return;
+    const double d = sqrt(d2);
+    const double ug = (m1 * si[0] + m2 * sj[0]) / (m1 + m2);
+    const double vg = (m1 * si[1] + m2 * sj[1]) / (m1 + m2);
+    const double ur = m1 * (si[0] - ug), vr = m1 * (si[1] - vg);
+    double vabs;
+    if (DIM == 3) {
+        const double wg = (m1 * si[2] + m2 * sj[2]) / (m1 + m2);
+        const double wr = m1 * (si[2] - wg);
+        vabs = (ur * ex + vr * ey + wr * ez) / d;
+    } else {
+        vabs = (ur * ex + vr * ey) / d;
+    }
+    if (!(vabs > 0)) return;
+    const double um = (1.0 + A.cc) * vabs * ex / d;
+    const double vm = (1.0 + A.cc) * vabs * ey / d;
+    const double wm = DIM == 3 ? (1.0 + A.cc) * vabs * ez / d : 0.0;
+    if (pti > 0) {
+        si[0] = si[0] - um / m1; si[1] = si[1] - vm / m1;
+        si[3] = si[3] - A.dt * um / m1; si[4] = si[4] - A.dt * vm / m1;
+        if (DIM == 3) { si[2] = si[2] - wm / m1; si[5] = si[5] - A.dt * wm / m1; }
+    }
+    if (ptj > 0) {
+        sj[0] = sj[0] + um / m2; sj[1] = sj[1] + vm / m2;
+        sj[3] = sj[3] + A.dt * um / m2; sj[4] = sj[4] + A.dt * vm / m2;
+        if (DIM == 3) { sj[2] = sj[2] + wm / m2; sj[5] = sj[5] + A.dt * wm / m2; }
+    }
+}
+
+// COLLISION2 (functions.cu:1523-1601) in an order-independent form.  The
+// reference walks every particle, walls and dummies included, in id order
+// and updates pairs in place, so a pair (a, b), a < b, is visited twice:
+// from a's list, then from b's list with the state the first visit left (a
+// fluid-wall pair can be pushed twice; a fluid-fluid pair separates after
+// the first push).  Each fluid particle here replays, for every neighbour
+// closer than coll in the pre-collision state, that pair's two visits in
+// registers.  With one such neighbour the particle takes the replayed state
+// -- COLLISION2's own result, bit for bit, as nothing else touches the pair
+// in between; with several it takes the pre-collision state plus the sum of
+// the pairs' changes.  The new states go to the *o arrays, and
+// k_collision_apply copies them over once every particle has read the
 // pre-collision state (no buffer swap, so the step's buffers stay fixed).
-// 4 resident blocks per SM (64 registers, 28 bytes of spills; 80 without the
-// bound): 0.02 ms per step faster on the 1.6 M-particle dam.
 template <int DIM, int G>
-__global__ void __launch_bounds__(256, 4) k_collision(int n, Lists L, CollArgs A, const int* __restrict__ ptype,
-                            const double4* __restrict__ P4, const double* __restrict__ un,
-                            const double* __restrict__ vn, const double* __restrict__ wn,
-                            double* __restrict__ dxo, double* __restrict__ dyo,
-                            double* __restrict__ dzo, double* __restrict__ duo,
-                            double* __restrict__ dvo, double* __restrict__ dwo)
+__global__ void __launch_bounds__(256, 3) k_collision(int n, Lists L, CollArgs A, const int* __restrict__ ptype,
+                            const int* __restrict__ oid, const double4* __restrict__ P4,
+                            const double* __restrict__ un, const double* __restrict__ vn,
+                            const double* __restrict__ wn, double* __restrict__ xo,
+                            double* __restrict__ yo, double* __restrict__ zo,
+                            double* __restrict__ uo, double* __restrict__ vo,
+                            double* __restrict__ wo)
 {
     Grp<G> q;
-    int i = (int)q.gid;
-    if (i >= n) return;
-    int pti = ptype[i];
+    const int i = (int)q.gid;
+    if (i >= n) return;  // whole groups leave together
+    const int pti = ptype[i];
     if (pti <= 0) return;
-    double4 pi = P4[i];
-    double ui = un[i], vi = vn[i], wi = DIM == 3 ? wn[i] : 0.0;
-    double du = 0, dv = 0, dw = 0, ddx = 0, ddy = 0, ddz = 0;
-    double m1 = (pti == 1) ? A.rho1 : A.rho2;
+    const double4 pi = P4[i];
+    const double s0[6] = {un[i], vn[i], DIM == 3 ? wn[i] : 0.0, pi.x, pi.y, DIM == 3 ? pi.z : 0.0};
+    // the replay of pair (i, j) into si
+    auto replay = [&](int j, const double4& pj, double* si) {
+        double sj[6] = {un[j], vn[j], DIM == 3 ? wn[j] : 0.0, pj.x, pj.y, DIM == 3 ? pj.z : 0.0};
+#pragma unroll
+        for (int t = 0; t < 6; t++) si[t] = s0[t];
+        const int ptj = ptype[j];
+        if (oid[j] < oid[i]) {
+            coll_visit<DIM>(A, ptj, pti, sj, si);
+            coll_visit<DIM>(A, pti, ptj, si, sj);
+        } else {
+            coll_visit<DIM>(A, pti, ptj, si, sj);
+            coll_visit<DIM>(A, ptj, pti, sj, si);
+        }
+    };
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    int hits = 0, jhit = -1;
     const int* row = row_of(L, i);
-    int len = L.len[i];
+    const int len = L.len[i];
     for (int k = q.lane; k < len; k += G) {
-        int j = row[k];
+        const int j = row[k];
         if (i == j) continue;
         double ex, ey, ez;
-        double d2 = d2of<DIM>(pi, P4[j], ex, ey, ez);
-        if (!(d2 < A.coll2)) continue;
-        double d = sqrt(d2);
-        double m2 = (ptype[j] == 1) ? A.rho1 : A.rho2;
-        double ug = (m1 * ui + m2 * un[j]) / (m1 + m2);
-        double vg = (m1 * vi + m2 * vn[j]) / (m1 + m2);
-        double ur = m1 * (ui - ug), vr = m1 * (vi - vg), vabs;
-        if (DIM == 3) {
-            double wg = (m1 * wi + m2 * wn[j]) / (m1 + m2);
-            double wr = m1 * (wi - wg);
-            vabs = (ur * ex + vr * ey + wr * ez) / d;
-        } else {
-            vabs = (ur * ex + vr * ey) / d;
-        }
-        if (!(vabs > 0)) continue;
-        double um = (1.0 + A.cc) * vabs * ex / d;
-        double vm = (1.0 + A.cc) * vabs * ey / d;
-        du -= um / m1; dv -= vm / m1;
-        ddx -= A.dt * um / m1; ddy -= A.dt * vm / m1;
-        if (DIM == 3) {
-            double wm = (1.0 + A.cc) * vabs * ez / d;
-            dw -= wm / m1; ddz -= A.dt * wm / m1;
-        }
+        const double4 pj = P4[j];
+        if (!(d2of<DIM>(pi, pj, ex, ey, ez) < A.coll2)) continue;
+        double si[6];
+        replay(j, pj, si);
+#pragma unroll
+        for (int t = 0; t < 6; t++) acc[t] += si[t] - s0[t];
+        hits++;
+        jhit = j;
     }
-    du = q.sum(du); dv = q.sum(dv); ddx = q.sum(ddx); ddy = q.sum(ddy);
-    if (DIM == 3) { dw = q.sum(dw); ddz = q.sum(ddz); }
+    int total = hits;
+    for (int o = G / 2; o > 0; o >>= 1) total += __shfl_xor_sync(q.mask, total, o);
+    double* const outs[6] = {uo, vo, wo, xo, yo, zo};
+    if (total == 1) {  // the lane that met the one neighbour writes its replayed state
+        if (hits == 1) {
+            double si[6];
+            replay(jhit, P4[jhit], si);
+            for (int t = 0; t < 6; t++)
+                if (DIM == 3 || (t != 2 && t != 5)) outs[t][i] = si[t];
+        }
+        return;
+    }
+    if (total > 1)
+#pragma unroll
+        for (int t = 0; t < 6; t++) acc[t] = q.sum(acc[t]);
     if (q.lane != 0) return;
-    dxo[i] = ddx; dyo[i] = ddy; duo[i] = du; dvo[i] = dv;
-    if (DIM == 3) { dzo[i] = ddz; dwo[i] = dw; }
+    for (int t = 0; t < 6; t++)
+        if (DIM == 3 || (t != 2 && t != 5)) outs[t][i] = total > 1 ? s0[t] + acc[t] : s0[t];
 }
 
 template <int DIM>
 __global__ void k_collision_apply(int n, const int* __restrict__ ptype, double* __restrict__ x,
                                   double* __restrict__ y, double* __restrict__ z,
                                   double* __restrict__ un, double* __restrict__ vn,
-                                  double* __restrict__ wn, const double* __restrict__ dx,
-                                  const double* __restrict__ dy, const double* __restrict__ dz,
-                                  const double* __restrict__ du, const double* __restrict__ dv,
-                                  const double* __restrict__ dw, double4* __restrict__ P4)
+                                  double* __restrict__ wn, const double* __restrict__ xo,
+                                  const double* __restrict__ yo, const double* __restrict__ zo,
+                                  const double* __restrict__ uo, const double* __restrict__ vo,
+                                  const double* __restrict__ wo, double4* __restrict__ P4)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || ptype[i] <= 0) return;
     double4 pi = P4[i];
-    pi.x = pi.x + dx[i];
-    pi.y = pi.y + dy[i];
+    pi.x = xo[i];
+    pi.y = yo[i];
     x[i] = pi.x;
     y[i] = pi.y;
-    un[i] = un[i] + du[i];
-    vn[i] = vn[i] + dv[i];
+    un[i] = uo[i];
+    vn[i] = vo[i];
     if (DIM == 3) {
-        pi.z = pi.z + dz[i];
+        pi.z = zo[i];
         z[i] = pi.z;
-        wn[i] = wn[i] + dw[i];
+        wn[i] = wo[i];
     }
     P4[i] = pi;
 }
@@ -1056,9 +1114,9 @@ int vmps_collision(mps_ctx* c)
 {
     const mps_config& f = c->cfg;
     CollArgs A{sqrt_cut(f.coll, true), f.cc, f.dt, f.rho1, f.rho2};
-    // deltas to the *c scratch arrays, then applied in place
-    LAUNCH_SMALL(k_collision, c->n, lists(c, 1), A, c->ptype, c->P4, c->un, c->vn, c->wn, c->xc,
-                 c->yc, c->zc, c->uc, c->vc, c->wc);
+    // new states to the *c scratch arrays, then copied over in place
+    LAUNCH_SMALL(k_collision, c->n, lists(c, 1), A, c->ptype, c->oid, c->P4, c->un, c->vn, c->wn,
+                 c->xc, c->yc, c->zc, c->uc, c->vc, c->wc);
     LAUNCH_DIM(k_collision_apply, c->n, c->ptype, c->x, c->y, c->z, c->un, c->vn, c->wn, c->xc,
                c->yc, c->zc, c->uc, c->vc, c->wc, c->P4);
     VMPS_CUDA(c, cudaGetLastError());
