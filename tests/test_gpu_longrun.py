@@ -3,43 +3,51 @@ collapse) on the CUDA path and on the oracle: the flow's integral
 quantities agree along the way.  Particle-level states drift apart slowly
 (sums in different orders, discrete collision and free-surface decisions),
 so the comparison is on the front position, the fluid's centroid and its
-kinetic energy.  The tolerances are set by the flow's own sensitivity: the
-oracle against itself with cg_tol 1e-8 and 1e-10 differs over the same run
-by up to 2.5% (front), 0.15% (centroid) and 1% (kinetic energy); the CUDA
-path measured 1.3%, 0.38% and 0.67%."""
+kinetic energy, every 200 steps.
+
+The bound is the flow's own sensitivity, measured in the test: the oracle
+run twice, at cg_tol 1e-8 and 1e-12, drifts apart by s (per quantity) --
+3.3% front, 0.12% centroid, 2.4% kinetic energy on this case.  The CUDA
+path (cg_tol 1e-8) must stay within 2 s of the oracle at the same
+tolerance, and never more than the fixed ceilings below."""
 import numpy as np
 import pytest
 
+import pyoracle
 from voxarmps_b200 import config
 from gpu_util import gpu_cfg, pair
 
 pytestmark = pytest.mark.gpu
 
-FRONT_TOL = 5e-2     # relative, front position (max x of the fluid)
-CENTROID_TOL = 1e-2  # relative, centroid y of the fluid
-KE_TOL = 3e-2        # relative, kinetic energy of the fluid
+FLOOR = (1e-2, 2e-3, 1e-2)     # the bound is never tighter than this (front, centroid, KE)
+CEILING = (1e-1, 1e-2, 6e-2)   # nor looser than this
 
 
 def _integrals(get, ptype):
     f = ptype > 0
     x, y, u, v = get("x")[f], get("y")[f], get("u")[f], get("v")[f]
-    return x.max(), y.mean(), 0.5 * (u * u + v * v).sum()
+    return np.array([x.max(), y.mean(), 0.5 * (u * u + v * v).sum()])
 
 
 def test_config0_whole_run_integrals():
     cfg, case = config.baseline(0)
     cfg = gpu_cfg(cfg)
     g, o = pair(cfg, case)
+    o12 = pyoracle.Oracle(gpu_cfg(cfg, cg_tol=1e-12), case)
+    assert o12.init() == 0
     pt = np.asarray(case["ptype"])
-    worst = [0.0, 0.0, 0.0]
+    gpu_dev = np.zeros(3)
+    self_dev = np.zeros(3)
     for k in range(2000):
         assert g.step() == 0
         o.step()
+        o12.step()
         if k % 200 == 199:
-            a, b = _integrals(g.get, pt), _integrals(o.get, pt)
-            for q in range(3):
-                worst[q] = max(worst[q], abs(a[q] - b[q]) / max(abs(b[q]), 1e-30))
-    print(f"\nworst relative differences over 2000 steps: front {worst[0]:.2e}, "
-          f"centroid {worst[1]:.2e}, kinetic energy {worst[2]:.2e}")
-    assert worst[0] <= FRONT_TOL and worst[1] <= CENTROID_TOL and worst[2] <= KE_TOL
+            a, b, c = _integrals(g.get, pt), _integrals(o.get, pt), _integrals(o12.get, pt)
+            gpu_dev = np.maximum(gpu_dev, np.abs(a - b) / np.abs(b))
+            self_dev = np.maximum(self_dev, np.abs(c - b) / np.abs(b))
+    bound = np.minimum(np.maximum(2 * self_dev, FLOOR), CEILING)
+    print(f"\nover 2000 steps (front, centroid, kinetic energy): CUDA vs oracle {gpu_dev}, "
+          f"oracle vs itself {self_dev}, bound {bound}")
+    assert np.all(gpu_dev <= bound), (gpu_dev, bound)
     g.close()

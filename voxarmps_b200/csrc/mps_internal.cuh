@@ -198,6 +198,11 @@ struct mps_ctx {
     int *bslot_s = nullptr, *boid_s = nullptr;
     int *src = nullptr, *inv = nullptr;            // new slot <- old slot, old -> new
     int *perm_s = nullptr, *perm_s_tmp = nullptr;  // small-grid cell order (slots)
+    // the PND-radius list is derived in the Laplacian list's pass (its
+    // support lies well inside the Laplacian radius); the PND grid's sort
+    // order is then only formed when it is downloaded
+    bool fuse_lists = false;
+    bool perm_s_valid = false;
     // lists (slot-major)
     int *nbr_l = nullptr, *len_l = nullptr, *nbr_s = nullptr, *len_s = nullptr;
     // PPE matrix (compact slot-major ELL) and CG vectors
@@ -447,6 +452,7 @@ int vmps_check(mps_ctx* ctx, cudaError_t e, const char* what);
 
 // stage launchers (defined in the kernel translation units)
 int vmps_neighbors(mps_ctx* ctx);
+int vmps_perm_s(mps_ctx* ctx);  // PND-grid order, formed on demand
 int vmps_pnd(mps_ctx* ctx, int at_star, int correct, int which_list, double* out);
 int vmps_max_reduce(mps_ctx* ctx, const double* a, double* result);
 int vmps_sps(mps_ctx* ctx);
