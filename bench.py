@@ -138,24 +138,25 @@ class ClockSampler:
 
 
 def spmv_algorithmic_bytes(nnz_a: float, rows: float) -> float:
-    """Bytes one FP64 CSR SpMV must move: per stored non-zero a column index
-    (4 B) and a value (8 B); per unknown row diag (8), length (4), offset (4),
-    bcon (4), the row's own p (8) and the written s (8).  Gathers of p_j are
-    L2 hits."""
-    return nnz_a * 12.0 + rows * 36.0
+    """Bytes one FP64 SpMV must move: per stored non-zero a 16-bit column code
+    (2 B) and a value (8 B); per unknown row its (offset, length) pair (8), its
+    nine run bases (36), diag (8), the row's own p (8) and the written s (8).
+    Gathers of p_j are L2 hits."""
+    return nnz_a * 10.0 + rows * 68.0
 
 
 def spmv32_algorithmic_bytes(nnz_a: float, rows: float) -> float:
     """Inner SpMV of the mixed-precision PPE: one (column, FP32 value) pair
-    (8 B) per non-zero; per row diag (8), length, offset, bcon (4 each), FP32
-    p and s (4 each)."""
-    return nnz_a * 8.0 + rows * 28.0
+    (8 B) per non-zero; per row (offset, length) (8), diag (8), FP32 p and s
+    (4 each)."""
+    return nnz_a * 8.0 + rows * 24.0
 
 
 def refine_algorithmic_bytes(nnz_a: float, rows: float) -> float:
-    """Refinement r -= A64 d, x += d: 12 B per non-zero; per row diag (8),
-    length, offset, bcon, FP32 d (4 each), r and x read and written (32)."""
-    return nnz_a * 12.0 + rows * 56.0
+    """Refinement r -= A64 d, x += d: 10 B per non-zero as the FP64 SpMV; per
+    row (offset, length) (8), run bases (36), diag (8), FP32 d (4), r and x
+    read and written (32)."""
+    return nnz_a * 10.0 + rows * 88.0
 
 
 WORKLOADS = {
@@ -202,25 +203,38 @@ def build_case(scale: int = 0, which: int = 1, precision=None, rank: int = 0, ws
     return cfg, case, scenes
 
 
-def cpu_reference_sample():
-    """Bounded CPU sample: 3D dam at the benchmark's spacing, 10x20x10 fluid in a
-    40x25x10 tank (12,608 particles), single support radius 4.0*l0 (the
-    reference has one radius for every stage)."""
+def cpu_reference_sample(scale: int = 1, radius: float = 4.0):
+    """Bounded CPU sample: 3D dam at the benchmark's spacing, a 10s x 20s x 10s
+    fluid column (scale 1: 12,608 particles) and one support radius for every
+    stage, as the reference has: 4.0*l0 (the Laplacian radius, so the PPE and
+    its IC(0) factorisation cost what they cost in the benchmark; the PND-list
+    stages then do more work than the GPU's 2.1*l0) or 2.1*l0 (every stage
+    cheaper than the GPU's)."""
     from voxarmps_b200 import config
-    cfg, case = config.scaled_dam3d(1)
+    cfg, case = config.scaled_dam3d(scale)
     cfg = dict(cfg)
-    cfg["re_s"] = cfg["re_l"] = 4.0 * cfg["l0"]
+    cfg["re_s"] = cfg["re_l"] = radius * cfg["l0"]
     return cfg, case
 
 
-def time_reference(steps: int, warmup: int, nthreads: int):
-    """The reference's own OpenMP CPU path (oracle/_ref/libref_omp.so); if it
-    was not built, the C restatement (single thread) stands in."""
+def physical_cores() -> int:
+    try:
+        import psutil
+        return int(psutil.cpu_count(logical=False) or os.cpu_count() or 1)
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def time_reference(steps: int, warmup: int, nthreads: int, scale: int = 1, radius: float = 4.0):
+    """The reference's own CPU path on a bounded sample: OpenMP
+    (oracle/_ref/libref_omp.so) with nthreads > 1, the sequential build
+    (libref.so) with 1; if it was not built, the C restatement (single
+    thread) stands in."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
-    cfg, case = cpu_reference_sample()
+    cfg, case = cpu_reference_sample(scale, radius)
     n = len(case["x"])
-    if pyoracle.ref_available(omp=True):
+    if pyoracle.ref_available(omp=nthreads > 1):
         kind, h = "reference", pyoracle.RefHarness(cfg, case, nthreads=nthreads)
         cores = nthreads
     else:
@@ -235,17 +249,68 @@ def time_reference(steps: int, warmup: int, nthreads: int):
         h.step()
     el = time.perf_counter() - t0
     h.close()
+    fl = int((np.asarray(case["ptype"]) > 0).sum())
+    col = "x".join(str(10 * scale * k) for k in (1, 2, 1))
     return {"value": n * steps / el, "unit": METRIC, "cores": cores, "kind": kind,
-            "sample": f"3D dam, l0=0.005, re=4.0*l0, {n} particles "
-                      f"(10x20x10 fluid), {steps} steps after {warmup} warm-up",
-            "ms_per_step": el / steps * 1e3}
+            "sample": f"3D dam, l0=0.005, one radius {radius}*l0 for every stage, {n} particles "
+                      f"({col} fluid, {fl}), {steps} steps after {warmup} warm-up, "
+                      f"{'OpenMP, ' + str(cores) + ' threads' if cores > 1 else 'sequential'}",
+            "ms_per_step": el / steps * 1e3, "particles": n}
+
+
+def cpu_series(nthreads: int):
+    """Around the headline CPU number: the same sample at the small radius,
+    a scaled series (scales 1-3 at 2.1*l0, where the reference's per-step
+    cost stays bounded) and the sequential build (OMP_NUM_THREADS=1 form)."""
+    out = {"physical_cores": physical_cores(), "logical_cpus": os.cpu_count()}
+    r = time_reference(3, 1, nthreads, 1, 2.1)
+    out["radius_2.1"] = {k: r[k] for k in ("value", "ms_per_step", "particles", "sample")}
+    out["scaled_2.1"] = []
+    for sc in (1, 2, 3):
+        r = time_reference(2 if sc < 3 else 1, 1 if sc < 3 else 0, nthreads, sc, 2.1)
+        out["scaled_2.1"].append({k: r[k] for k in ("value", "ms_per_step", "particles")})
+    r = time_reference(1, 0, 1, 1, 4.0)
+    out["sequential_4.0"] = {k: r[k] for k in ("value", "ms_per_step", "particles", "sample",
+                                                 "kind")}
+    out["solver_iterations"] = solver_iterations()
+    return out
+
+
+def solver_iterations():
+    """Iterations to the 1e-8 relative residual of the reference's ICCG
+    (IC(0) preconditioner) against the Jacobi-PCG the GPU runs and plain CG,
+    on the same PPE systems (the oracle's, from the previous pressure), for
+    the 2D dam break after 20 steps and a 3D dam at the benchmark's spacing
+    and radii after 10 steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from voxarmps_b200 import cases, config
+    out = {}
+    c3 = cases.dam_break(3, 0.005, (6, 10, 6), (20, 14, 8))
+    f3 = config.reference_defaults(0.005, 3)
+    f3.update(re_s=2.1 * 0.005, re_l=4.0 * 0.005, dt=5e-5, gy=-9.81)
+    for name, (cfg, case), steps in (("dam2d_config0_step20", config.baseline(0), 20),
+                                     ("dam3d_6x10x6_step10", (config.with_box(f3, c3), c3), 10)):
+        cfg = config.solver_semantics(cfg)
+        o = pyoracle.Oracle(cfg, case)
+        o.init()
+        prev = None
+        for _ in range(steps):
+            prev = o.get("p")
+            o.step()
+        off, nbr, bcon, diag, val, b, _p = pyoracle.ppe_system(cfg, o)
+        it = pyoracle.solver_iterations(off, nbr, bcon, diag, val, b, prev)
+        out[name] = {"unknowns": int((bcon == 0).sum()), "iccg": it["iccg"],
+                     "jacobi_pcg": it["jacobi"], "cg": it["plain"], "tol": 1e-8}
+        o.close()
+    return out
 
 
 def run_reference_arm(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    nthreads = os.cpu_count() or 1
+    nthreads = physical_cores()
     r = time_reference(args.steps, args.warmup, nthreads)
     line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": METRIC,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -388,9 +453,34 @@ def run_ours(args):
     # its traffic/algorithmic ratio); not captured for the mixed kernel
     traffic = None if mixed else SPMV_TRAFFIC_OVER_ALGORITHMIC * algo
     line = None
+    # ---- the flow's later state: untimed steps to step `advanced`, then K
+    # steps timed as above (the early steps are the easiest window) ----
+    adv = None
+    if args.advanced and args.config in (1, 2) and not args.scale:
+        s.set_graph(bool(args.graph))
+        done = int(s.scalar("steps"))
+        for _ in range(max(0, args.advanced - done)):
+            s.step()
+        barrier()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ait = []
+        a0.record(stream)
+        for _ in range(args.steps):
+            status |= s.step()
+            ait.append(s.scalar("cg_iters"))
+        a1.record(stream)
+        barrier()
+        adv_ms = rank_max(a0.elapsed_time(a1)) / args.steps
+        adv = {"after_steps": max(args.advanced, done), "ms_per_step": adv_ms,
+               "value": n * 1e3 / adv_ms * (ws if not split else 1),
+               "cg_iters_mean": statistics.mean(ait)}
     if rank == 0:
-        cpu = (time_reference(steps=3, warmup=1, nthreads=os.cpu_count() or 1)
-               if ws == 1 and args.config in (1, 2) and not args.scale else None)
+        cpu = None
+        if ws == 1 and args.config in (1, 2) and not args.scale:
+            nth = physical_cores()
+            cpu = time_reference(steps=3, warmup=1, nthreads=nth)
+            if args.cpu_series:
+                cpu["series"] = cpu_series(nth)
     # units of the whole job: a split batch counts every rank's own particles
     n_job = sum_over_ranks(float(n), ws) if split else float(n) * ws
     fp_job = sum_over_ranks(float(fp), ws) if split else float(fp) * ws
@@ -435,9 +525,12 @@ def run_ours(args):
             "e2e": {"value": whole_job_rate(n_job * args.steps, 1, e2e_ms), "unit": METRIC,
                     "h2d_bytes_per_step": bytes_state, "d2h_bytes_per_step": bytes_state},
             "gpu_launches": launches, "clocks": clocks,
-            "cpu_baseline": ({k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            "cpu_baseline": ({k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                                  "series") if k in cpu}
                              if cpu else None),
         }
+        if adv:
+            line["advanced"] = adv
     s.close()
     if line is not None and mixed:
         line["error_vs_fp64"] = mixed_vs_fp64(vm, cfg, case, scenes, dev, steps=10)
@@ -585,6 +678,10 @@ def main():
                     help="benchmark configuration (1: the headline 3D dam break)")
     ap.add_argument("--advance", type=int, default=0,
                     help="profiling only: untimed steps before autotuning and warm-up")
+    ap.add_argument("--advanced", type=int, default=500,
+                    help="configs 1/2: also time K steps after this many steps (0: skip)")
+    ap.add_argument("--cpu-series", type=int, default=1, choices=[0, 1],
+                    help="configs 1/2: CPU baseline at the small radius, scaled and sequential")
     ap.add_argument("--scale", type=int, default=0,
                     help="profiling only: smaller 3D dam (10s x 20s x 10s fluid)")
     args = ap.parse_args()

@@ -447,6 +447,61 @@ int mo_cgm_ref(const mo_params* P, int n, const int* off, const int* nbr, const 
     return iters;
 }
 
+/* The reference's ICCG iteration (functions.cu:506-716: IC(0) factor from
+   INCDECOM, forward and backward substitution as preconditioner) stopped on
+   the relative residual ||b-Ax||/||b|| <= tol like mo_cg, so that its
+   iteration count compares with the Jacobi-PCG of the CUDA path at the same
+   tolerance.  Rows with bcon != 0 are held at 0. */
+int mo_iccg(int n, const int* off, const int* nbr, const int* bcon, const double* diag,
+            const double* val, const double* icd, const double* icv, const double* b, double* x,
+            double tol, int maxit, double* relres_out)
+{
+    size_t sz = sizeof(double) * (size_t)(n > 0 ? n : 1);
+    double* r = (double*)calloc(1, sz);
+    double* p = (double*)calloc(1, sz);
+    double* q = (double*)calloc(1, sz);
+    double* s = (double*)calloc(1, sz);
+    double* aux = (double*)calloc(1, sz);
+    for (int i = 0; i < n; i++) if (bcon[i] != 0) x[i] = 0.0;
+    mo_spmv(n, off, nbr, bcon, diag, val, x, s);
+    double bb = 0.0, rr = 0.0;
+    for (int i = 0; i < n; i++) {
+        if (bcon[i] != 0) continue;
+        r[i] = b[i] - s[i];
+        bb += b[i] * b[i];
+        rr += r[i] * r[i];
+    }
+    ic_solve(n, off, nbr, bcon, icd, icv, r, q, aux);
+    for (int i = 0; i < n; i++) p[i] = bcon[i] == 0 ? q[i] : 0.0;
+    double rq = 0.0;
+    for (int i = 0; i < n; i++) if (bcon[i] == 0) rq += r[i] * q[i];
+    int it = 0;
+    const double thr = tol * tol * bb;
+    while (rr > thr && it < maxit) {
+        mo_spmv(n, off, nbr, bcon, diag, val, p, s);
+        double ps = 0.0;
+        for (int i = 0; i < n; i++) if (bcon[i] == 0) ps += p[i] * s[i];
+        double a = rq / ps;
+        rr = 0.0;
+        for (int i = 0; i < n; i++) {
+            if (bcon[i] != 0) continue;
+            x[i] += a * p[i];
+            r[i] -= a * s[i];
+            rr += r[i] * r[i];
+        }
+        ic_solve(n, off, nbr, bcon, icd, icv, r, q, aux);
+        double rqn = 0.0;
+        for (int i = 0; i < n; i++) if (bcon[i] == 0) rqn += r[i] * q[i];
+        double beta = rqn / rq;
+        rq = rqn;
+        for (int i = 0; i < n; i++) if (bcon[i] == 0) p[i] = q[i] + beta * p[i];
+        it++;
+    }
+    if (relres_out) *relres_out = mo_relres(n, off, nbr, bcon, diag, val, b, x);
+    free(r); free(p); free(q); free(s); free(aux);
+    return it;
+}
+
 double mo_relres(int n, const int* off, const int* nbr, const int* bcon, const double* diag,
                  const double* val, const double* b, const double* x)
 {

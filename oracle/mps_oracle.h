@@ -107,6 +107,9 @@ int mo_cgm_ref(const mo_params* P, int n, const int* off, const int* nbr, const 
 int mo_cg(int n, const int* off, const int* nbr, const int* bcon, const double* diag,
           const double* val, const double* b, double* x, double tol, int maxit, int precond,
           double* relres_out);
+int mo_iccg(int n, const int* off, const int* nbr, const int* bcon, const double* diag,
+            const double* val, const double* icd, const double* icv, const double* b, double* x,
+            double tol, int maxit, double* relres_out);
 void mo_spmv(int n, const int* off, const int* nbr, const int* bcon, const double* diag,
              const double* val, const double* xin, double* s);
 double mo_relres(int n, const int* off, const int* nbr, const int* bcon, const double* diag,

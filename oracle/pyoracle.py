@@ -119,6 +119,10 @@ def _load_oracle():
                               _IP, _IP, _DP, _DP, _DP, _IP, _DP, _DP]
     lib.mo_lambda.restype = C.c_double
     lib.mo_lambda.argtypes = [C.c_int, C.c_double]
+    lib.mo_incdecom.argtypes = [C.c_int, _IP, _IP, _IP, _DP, _DP, _DP, _DP]
+    lib.mo_iccg.restype = C.c_int
+    lib.mo_iccg.argtypes = [C.c_int, _IP, _IP, _IP, _DP, _DP, _DP, _DP, _DP, _DP, C.c_double,
+                            C.c_int, _DP]
     for name in ("mo_collision", "mo_collision_gather"):
         getattr(lib, name).argtypes = [C.POINTER(MoParams), C.c_int, _IP, _IP, _IP, _DP, _DP,
                                        _DP, _DP, _DP, _DP]
@@ -273,6 +277,44 @@ def collision(cfg: dict, off, nbr, ptype, un, vn, wn, x, y, z, gather: bool = Fa
        _ip(np.ascontiguousarray(nbr, np.int32)), _ip(np.ascontiguousarray(ptype, np.int32)),
        *[_dp(v) for v in a])
     return tuple(a)
+
+
+def ppe_system(cfg: dict, o: "Oracle"):
+    """The PPE system of the oracle's last step: (off, nbr, bcon, diag, val, b,
+    p) with A assembled at the predicted positions on the Laplacian list, as
+    the step solved it (functions.cu:869-1133)."""
+    lib = oracle_lib()
+    P = params_from(cfg)
+    n = o.n
+    off, nbr = o.get("off_l"), o.get("nbr_l")
+    xs, ys, zs = o.get("xs"), o.get("ys"), o.get("zs")
+    bcon, b, p = o.get("bcon"), o.get("source"), o.get("pnew")
+    diag, val = np.zeros(n), np.zeros(max(len(nbr), 1))
+    lib.mo_matrix(C.byref(P), cfg["re_l"], lib.mo_lambda(cfg["ktype"], cfg["re_l"]),
+                  o.scalar("n0_l"), n, _ip(off), _ip(nbr), _dp(xs), _dp(ys), _dp(zs), _ip(bcon),
+                  _dp(diag), _dp(val))
+    return off, nbr, bcon, diag, val, b, p
+
+
+def solver_iterations(off, nbr, bcon, diag, val, b, x0, tol=1e-8, maxit=5000):
+    """Iterations to ||b-Ax||/||b|| <= tol from x0: the reference's ICCG
+    (IC(0) preconditioner) against Jacobi-PCG and plain CG."""
+    lib = oracle_lib()
+    n = len(diag)
+    out = {}
+    icd, icv = np.zeros(n), np.zeros(max(len(nbr), 1))
+    lib.mo_incdecom(n, _ip(off), _ip(nbr), _ip(bcon), _dp(diag), _dp(val), _dp(icd), _dp(icv))
+    rr = C.c_double()
+    x = np.array(x0, np.float64)
+    out["iccg"] = lib.mo_iccg(n, _ip(off), _ip(nbr), _ip(bcon), _dp(diag), _dp(val), _dp(icd),
+                              _dp(icv), _dp(b), _dp(x), tol, maxit, C.byref(rr))
+    out["iccg_relres"] = rr.value
+    for name, pre in (("jacobi", 1), ("plain", 0)):
+        x = np.array(x0, np.float64)
+        out[name] = lib.mo_cg(n, _ip(off), _ip(nbr), _ip(bcon), _dp(diag), _dp(val), _dp(b),
+                              _dp(x), tol, maxit, pre, C.byref(rr))
+        out[name + "_relres"] = rr.value
+    return out
 
 
 def W(r, ktype, dim, re):

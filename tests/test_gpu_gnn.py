@@ -15,11 +15,14 @@ from gpu_util import gpu_cfg, oracle_relres
 pytestmark = pytest.mark.gpu
 
 L = 4
-# forward: identical rounding points and summation order; the bound allows
-# for the library's FP32 division differing in the last bit
-Y_TOL = 1e-5
-# gradient: FP32 sums in a different order than the FP64 oracle
-GRAD_TOL = 2e-3
+# forward: the layer products run on the tensor cores, which sum the 128
+# products of a row in their own order (FP32); an activation rounded to BF16
+# can then land one BF16 unit (2^-8 relative) away from the oracle's, and
+# four layers carry that forward
+Y_TOL = 1e-2
+# gradient: FP32 sums in a different order than the FP64 oracle, on the
+# tensor-core forward's activations
+GRAD_TOL = 1e-2
 
 
 def _ctx(steps=2, seed=7, scale=0.1):
@@ -48,7 +51,9 @@ def test_forward_matches_oracle():
     feat, nbr, ln, cap = _graph(s)
     y = s.gnn_get("y")
     ref = G.forward(p, feat, nbr, ln, cap, L)["y"]
-    assert np.abs(y - ref).max() <= Y_TOL * max(np.abs(ref).max(), 1e-30)
+    err = np.abs(y - ref).max() / max(np.abs(ref).max(), 1e-30)
+    print(f"\nforward: max |y - y_oracle| / max |y_oracle| = {err:.3e}")
+    assert err <= Y_TOL
     s.close()
 
 
@@ -68,6 +73,7 @@ def test_gradient_matches_oracle():
     blocks += [(f"W{l}", lay["W"][l], lay["b"][l] + G.H) for l in range(L)]
     for name, a, b in blocks:
         err = np.linalg.norm(g[a:b] - gref[a:b]) / max(np.linalg.norm(gref[a:b]), 1e-30)
+        print(f"gradient {name}: relative error {err:.3e}")
         assert err <= GRAD_TOL, (name, err)
     s.close()
 

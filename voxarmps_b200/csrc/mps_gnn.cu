@@ -17,14 +17,14 @@
 //   y   = wd . h_L + bd,   guess = p_prev + pref * y   (unknown rows)
 // with pref = max(rms of p_prev over the unknown rows, rho1 |g| l0).
 //
-// Precision: weights and activations are stored in BF16; every sum
-// accumulates in FP32 in a fixed sequential order (so a CPU restatement can
-// reproduce the forward pass).  Training keeps FP32 master weights, takes
-// Adam steps on the mean squared error of y against the solved increment
-// (p_solved - p_prev) / pref over the unknown fluid rows, and reduces weight
-// gradients through fixed per-block partials (deterministic).  All kernels
-// are CUDA-core code: the per-node products are 64 x 128 at most, far too
-// small to occupy tensor cores.
+// Precision: weights and activations are stored in BF16; sums accumulate
+// in FP32.  Each layer's product W [h, m] is one [nodes x 128] x [128 x 64]
+// BF16 GEMM on the tensor cores (tcgen05.mma, FP32 accumulator in tensor
+// memory, k_gnn_layer_tc); the aggregation, encoder, decoder and the
+// backward pass are CUDA-core kernels with sums in a fixed order.  Training
+// keeps FP32 master weights, takes Adam steps on the chosen objective and
+// reduces weight gradients through fixed per-block partials
+// (deterministic).
 #include <cuda_bf16.h>
 
 #include "mps_internal.cuh"
@@ -205,45 +205,199 @@ __global__ void k_gnn_agg(int n, int cap, const int* __restrict__ nbr, const int
     *(bf162*)(mout + (size_t)i * H + 2 * q.lane) = __floats2bfloat162_rn(s0, s1);
 }
 
-// h_out = h_in + relu(W [h_in, m] + b); warp per node; W^T staged in shared
-// memory as FP32, the node's 128 inputs staged per warp
-__global__ void __launch_bounds__(kThreads) k_gnn_layer(int n, const bf16* __restrict__ w16, int offW,
-                                                        int offb, const bf16* __restrict__ hin,
-                                                        const bf16* __restrict__ min_,
-                                                        bf16* __restrict__ hout, bf16* __restrict__ zout)
+// ---- the layer on the tensor cores ---------------------------------------
+// h_out = h_in + relu(W [h_in, m] + b), z_out = W [h_in, m] + b for 128 nodes
+// at a time: the node tile [h, m] (128 x 128 BF16) and W (64 x 128 BF16) sit
+// in shared memory, one thread issues a chain of eight tcgen05.mma (K = 16
+// each) into a 128 x 64 FP32 accumulator in tensor memory (node r in TMEM
+// lane r), and four warps -- one per 32 lanes -- read it back for the bias,
+// ReLU and residual epilogue.  Blocks loop over the node tiles.
+constexpr int kTcM = 128;          // nodes per tile, the MMA's M
+constexpr int kTcK = 2 * H;        // the inputs [h, m]
+constexpr int kTcThreads = 128;    // four warps
+constexpr uint32_t kTcCols = 64;   // TMEM columns of the accumulator (N = H)
+constexpr unsigned kTcWaitLimit = 1u << 22;  // mbarrier polls before giving up
+
+struct TcSmem {
+    unsigned char a[kTcM * kTcK * 2];  // node tile, core-matrix layout (32 KB)
+    unsigned char w[H * kTcK * 2];     // W, core-matrix layout (16 KB)
+    float bias[H];
+    unsigned long long bar;            // MMA completion
+    uint32_t tmem;                     // accumulator address from tcgen05.alloc
+};
+constexpr size_t kTcSmemBytes = sizeof(TcSmem) + 128;
+
+// Byte offset of element (r, k) of an R-row, K-major BF16 operand in the
+// no-swizzle layout of tcgen05: core matrices of 8 rows x 16 bytes (8 K
+// values) are 128 contiguous bytes; the R/8 core matrices of one 8-wide K
+// chunk follow one another, then the next K chunk.  Core matrices adjacent
+// in K are R*16 bytes apart (the descriptor's leading byte offset), adjacent
+// in rows 128 bytes apart (its stride byte offset).
+__device__ __forceinline__ uint32_t core_offset(int r, int k, int R)
 {
-    __shared__ float Wt[2 * H][H];  // Wt[k][c] = W[c][k]
-    __shared__ float us[kThreads / 32][2 * H];
-    __shared__ float bs[H];
-    for (int e = threadIdx.x; e < 2 * H * H; e += blockDim.x) {
-        const int c = e / (2 * H), k = e % (2 * H);
-        Wt[k][c] = __bfloat162float(w16[offW + e]);
+    return (uint32_t)(((((k >> 3) * (R >> 3)) + (r >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1));
+}
+
+// tcgen05 shared-memory matrix descriptor: start address, leading and stride
+// byte offsets (each in 16-byte units), descriptor version 1 (bits 46-47),
+// base offset 0, no swizzling
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor of kind::f16: D in FP32 (bits 4-5 = 1), A and B in
+// BF16 (bits 7-9 and 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at
+// bit 24
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(H >> 3) << 17) |
+                              ((uint32_t)(kTcM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// bounded wait for the given phase parity of an mbarrier
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    for (unsigned it = 0; it < kTcWaitLimit; it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
     }
-    for (int c = threadIdx.x; c < H; c += blockDim.x) bs[c] = __bfloat162float(w16[offb + c]);
+    return false;
+}
+
+__global__ void __launch_bounds__(kTcThreads) k_gnn_layer_tc(
+    int n, const bf16* __restrict__ w16, int offW, int offb, const bf16* __restrict__ hin,
+    const bf16* __restrict__ min_, bf16* __restrict__ hout, bf16* __restrict__ zout,
+    unsigned int* err)
+{
+    extern __shared__ unsigned char tc_raw[];
+    TcSmem& S = *reinterpret_cast<TcSmem*>((reinterpret_cast<uintptr_t>(tc_raw) + 127) &
+                                           ~(uintptr_t)127);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t a_addr = smem_addr(S.a), w_addr = smem_addr(S.w), bar = smem_addr(&S.bar);
+    // W[c][k] (row-major, K fastest) into the core-matrix layout, 16 bytes at a time
+    for (int e = tid; e < H * (kTcK / 8); e += kTcThreads) {
+        const int c = e / (kTcK / 8), k8 = e % (kTcK / 8);
+        const uint4 v = *reinterpret_cast<const uint4*>(w16 + offW + c * kTcK + k8 * 8);
+        *reinterpret_cast<uint4*>(S.w + core_offset(c, k8 * 8, H)) = v;
+    }
+    for (int c = tid; c < H; c += kTcThreads) S.bias[c] = __bfloat162float(w16[offb + c]);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_addr(&S.tmem)),
+                     "r"(kTcCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int nw = gridDim.x * (blockDim.x >> 5);
-    float* u = us[wib];
-    for (int i = blockIdx.x * (blockDim.x >> 5) + wib; i < n; i += nw) {
-        const size_t o = (size_t)i * H + 2 * lane;
-        const float2 hv = __bfloat1622float2(*(const bf162*)(hin + o));
-        const float2 mv = __bfloat1622float2(*(const bf162*)(min_ + o));
-        u[2 * lane] = hv.x;
-        u[2 * lane + 1] = hv.y;
-        u[H + 2 * lane] = mv.x;
-        u[H + 2 * lane + 1] = mv.y;
-        __syncwarp();
-        float a0 = bs[2 * lane], a1 = bs[2 * lane + 1];
-        for (int k = 0; k < 2 * H; k++) {
-            const float uk = u[k];
-            const float2 w = *(const float2*)&Wt[k][2 * lane];
-            a0 = a0 + w.x * uk;
-            a1 = a1 + w.y * uk;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = S.tmem;
+    const int tiles = (n + kTcM - 1) / kTcM;
+    uint32_t parity = 0;
+    bool failed = false;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const int node0 = t * kTcM;
+        // [h, m] of the tile's nodes; rows past n are zero
+        for (int e = tid; e < kTcM * (kTcK / 8); e += kTcThreads) {
+            const int k8 = e / kTcM, r = e % kTcM, node = node0 + r;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (node < n)
+                v = *reinterpret_cast<const uint4*>(k8 < H / 8 ? hin + (size_t)node * H + k8 * 8
+                                                             : min_ + (size_t)node * H + (k8 - H / 8) * 8);
+            *reinterpret_cast<uint4*>(S.a + core_offset(r, k8 * 8, kTcM)) = v;
         }
-        __syncwarp();
-        *(bf162*)(zout + o) = __floats2bfloat162_rn(a0, a1);
-        *(bf162*)(hout + o) = __floats2bfloat162_rn(hv.x + fmaxf(a0, 0.f), hv.y + fmaxf(a1, 0.f));
+        // the tile's shared-memory writes become visible to the tensor cores
+        asm volatile("fence.proxy.async.shared::cta;");
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (tid == 0) {
+#pragma unroll
+            for (int s = 0; s < kTcK / 16; s++) {
+                const uint64_t ad = umma_desc(a_addr + s * 2 * (kTcM * 16), kTcM * 16, 128);
+                const uint64_t bd = umma_desc(w_addr + s * 2 * (H * 16), H * 16, 128);
+                const uint32_t acc = s > 0 ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                    :
+                    : "r"(tmem), "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(acc), "r"(0u), "r"(0u),
+                      "r"(0u), "r"(0u));
+            }
+            asm volatile(
+                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                    bar));
+        }
+        failed = !mbar_wait(bar, parity);
+        parity ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (__syncthreads_or(failed)) {
+            failed = true;
+            break;
+        }
+        // epilogue: node r of the tile is TMEM lane r, warp w reads lanes 32w..32w+31
+        const int r = warp * 32 + lane, node = node0 + r;
+#pragma unroll
+        for (int cb = 0; cb < H; cb += 16) {
+            uint32_t v[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                  "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                  "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (node < n) {
+                __align__(16) bf16 zo[16], ho[16];
+#pragma unroll
+                for (int j = 0; j < 16; j++) {
+                    const int c = cb + j;
+                    const float zv = __uint_as_float(v[j]) + S.bias[c];
+                    const float hv = __bfloat162float(
+                        *reinterpret_cast<const bf16*>(S.a + core_offset(r, c, kTcM)));
+                    zo[j] = __float2bfloat16_rn(zv);
+                    ho[j] = __float2bfloat16_rn(hv + fmaxf(zv, 0.f));
+                }
+                const size_t o = (size_t)node * H + cb;
+                if (zout) {
+                    *reinterpret_cast<uint4*>(zout + o) = *reinterpret_cast<const uint4*>(zo);
+                    *reinterpret_cast<uint4*>(zout + o + 8) = *reinterpret_cast<const uint4*>(zo + 8);
+                }
+                *reinterpret_cast<uint4*>(hout + o) = *reinterpret_cast<const uint4*>(ho);
+                *reinterpret_cast<uint4*>(hout + o + 8) = *reinterpret_cast<const uint4*>(ho + 8);
+            }
+        }
+        // the tile's shared memory and accumulator are free again
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;");
     }
+    if (failed) {
+        // an MMA that never signalled: flag it, give it one more bounded wait
+        // before its accumulator is released
+        if (tid == 0) atomicOr(err, (unsigned)MPS_ERR_CUDA);
+        mbar_wait(bar, parity ^ 1u);
+    }
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kTcCols));
 }
 
 // y = bd + wd . h_L, sequential over channels; thread per node
@@ -635,6 +789,18 @@ int features(mps_ctx* c, vmps_gnn* G)
     return MPS_OK;
 }
 
+// the tensor-core layer needs more than the default 48 KB of dynamic shared
+// memory; set once per device, outside any stream capture
+int tc_prepare(mps_ctx* c)
+{
+    static bool done[64] = {};
+    if (c->device >= 0 && c->device < 64 && done[c->device]) return MPS_OK;
+    VMPS_CUDA(c, cudaFuncSetAttribute(k_gnn_layer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kTcSmemBytes));
+    if (c->device >= 0 && c->device < 64) done[c->device] = true;
+    return MPS_OK;
+}
+
 int forward(mps_ctx* c, vmps_gnn* G)
 {
     const int n = c->n;
@@ -645,13 +811,14 @@ int forward(mps_ctx* c, vmps_gnn* G)
     vmps_count_launch(1);
     int sms = 0;
     VMPS_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-    const int lblocks = std::max(1, std::min(warp_blocks(n), sms * 4));
+    // node tiles of the tensor-core layer: up to three resident blocks per SM
+    const int tc_blocks = std::max(1, std::min((n + kTcM - 1) / kTcM, sms * 3));
     for (int l = 0; l < Y.L; l++) {
         k_gnn_agg<<<warp_blocks(n), kThreads, 0, st>>>(n, c->cap_s, c->nbr_s, c->len_s,
                                                        G->h + l * NH, G->mm + l * NH);
-        k_gnn_layer<<<lblocks, kThreads, 0, st>>>(n, G->w16, Y.W[l], Y.b[l], G->h + l * NH,
-                                                  G->mm + l * NH, G->h + (l + 1) * NH,
-                                                  G->z + (l + 1) * NH);
+        k_gnn_layer_tc<<<tc_blocks, kTcThreads, kTcSmemBytes, st>>>(
+            n, G->w16, Y.W[l], Y.b[l], G->h + l * NH, G->mm + l * NH, G->h + (l + 1) * NH,
+            G->z + (l + 1) * NH, c->d_err);
         vmps_count_launch(2);
     }
     k_gnn_dec<<<grid_blocks(n), kThreads, 0, st>>>(n, G->w16, Y, G->h + Y.L * NH, G->y);
@@ -805,6 +972,7 @@ int mps_gnn_create(mps_ctx* c, int layers, unsigned long long seed)
     GTRY(galloc(c, G, &G->v, P));
     GTRY(galloc(c, G, &G->g, P));
     GTRY(galloc(c, G, &G->w16, P));
+    GTRY(tc_prepare(c));
     GTRY(galloc(c, G, &G->part, (size_t)kWgradBlocks * kMaxE));
     GTRY(galloc(c, G, &G->red, (size_t)2 * kWgradBlocks));
     GTRY(galloc(c, G, &G->scal, 4));

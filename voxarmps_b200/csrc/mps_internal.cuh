@@ -205,8 +205,11 @@ struct mps_ctx {
     bool perm_s_valid = false;
     // lists (slot-major)
     int *nbr_l = nullptr, *len_l = nullptr, *nbr_s = nullptr, *len_s = nullptr;
-    // PPE matrix (compact slot-major ELL) and CG vectors
-    int *mcol = nullptr, *mlen = nullptr, *moff = nullptr;  // CSR: row i at moff[i]
+    int* lbase = nullptr;  // first slot of each run of a Laplacian row (kLapRuns per row)
+    // PPE matrix (compact slot-major CSR: row i at moff[i]) and CG vectors;
+    // columns as 16-bit (run, offset) codes against lbase
+    unsigned short* mcode = nullptr;
+    int *mlen = nullptr, *moff = nullptr;
     int2* mrow = nullptr;  // (moff, mlen) per row, mlen -1 for rows outside the system
     double* mval = nullptr;
     double *pres_x = nullptr, *pres_y = nullptr, *pres_z = nullptr;  // prediction pressure sums
@@ -326,6 +329,29 @@ __device__ __forceinline__ bool cell_coords(const Grid& g, double x, double y, d
 }
 
 inline int grid_blocks(long n) { return (int)((n + kBlock - 1) / kBlock); }
+
+// Laplacian-list entries: bits 0-27 the neighbour's slot, bits 28-31 the
+// run of cells (one (y, z) offset's x-triple, kLapRuns per row) in which the
+// list pass found it; kLapRuns first slots per row (lbase) go with them.  The
+// PPE matrix codes each column as (run, slot - first slot of the run) in 16
+// bits.
+constexpr int kSlotBits = 28;
+constexpr unsigned kSlotMask = (1u << kSlotBits) - 1u;
+constexpr int kLapRuns = 9;
+constexpr int kRunOffBits = 12;
+constexpr unsigned kRunOffMask = (1u << kRunOffBits) - 1u;
+
+// The w slot of the FP32 positions (P4f): bits 0-1 the particle kind + 1
+// (PTYPE -1..2), bits 2-11, 12-21, 22-31 the 0-based x, y, z cell of the
+// particle on the PND grid (each axis at most 1024 cells when it is used).
+__host__ __device__ __forceinline__ unsigned pnd_cell_word(int ptype, int cell, int ncx, int ncxy)
+{
+    const int c = cell - 1;
+    const unsigned a = (unsigned)(c % ncx), b = (unsigned)((c % ncxy) / ncx),
+                   k = (unsigned)(c / ncxy);
+    return (unsigned)(ptype + 1) | ((a & 1023u) << 2) | ((b & 1023u) << 12) | ((k & 1023u) << 22);
+}
+__device__ __forceinline__ int pnd_word_ptype(float w) { return (int)(__float_as_uint(w) & 3u) - 1; }
 
 // W() of functions.cu:32-74 from d2 and rD = rsqrt(d2)
 template <int DIM>

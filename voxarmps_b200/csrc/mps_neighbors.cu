@@ -356,24 +356,26 @@ __global__ void __launch_bounds__(256, 8) k_lists(int n, Grid g, double cut, flo
 // at the PND cutoff and sits in one of the 3x3(x3) PND-grid cells around i's
 // (functions.cu:2854-2918 on the PND grid; in 3D that cell rule is not implied
 // by the distance, x/y cells being re wide under a cutoff of re + DELTA).
+// The cell test reads the PND-grid cells packed with the positions, so it
+// adds no load to the candidate loop.
 struct SmallSide {
     double cut;         // squared-distance threshold (3D <=, 2D <)
     float lo, hi;       // FP32 screening window around cut
     int cap;            // row capacity
     int* out;           // rows, i * cap
     int* len;           // row lengths
-    const int* cell;    // PND-grid cell number of every slot (1-based)
-    int ncx, ncxy;      // PND grid: cells along x, cells per z layer
 };
 
-__device__ __forceinline__ bool pnd_cells_adjacent(const SmallSide& S, int ci, int cj)
+// PND-grid cells of two particles within one cell of each other along every
+// axis; the cells come packed in the w slot of their FP32 positions
+// (pnd_cell_word)
+__device__ __forceinline__ bool pnd_cells_adjacent(float wi, float wj)
 {
-    ci -= 1;
-    cj -= 1;
-    const int ai = ci % S.ncx, aj = cj % S.ncx;
-    const int bi = (ci % S.ncxy) / S.ncx, bj = (cj % S.ncxy) / S.ncx;
-    const int ki = ci / S.ncxy, kj = cj / S.ncxy;
-    return abs(ai - aj) <= 1 && abs(bi - bj) <= 1 && abs(ki - kj) <= 1;
+    const unsigned a = __float_as_uint(wi), b = __float_as_uint(wj);
+    const int dx = (int)((a >> 2) & 1023u) - (int)((b >> 2) & 1023u);
+    const int dy = (int)((a >> 12) & 1023u) - (int)((b >> 12) & 1023u);
+    const int dz = (int)(a >> 22) - (int)(b >> 22);
+    return abs(dx) <= 1 && abs(dy) <= 1 && abs(dz) <= 1;
 }
 
 // The same lists for Q particles of one cell at a time, one warp: each
@@ -393,7 +395,7 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
                                           const int* __restrict__ cst, const int* __restrict__ cnt,
                                           int* __restrict__ out, int* __restrict__ len,
                                           int* len_max, int which, unsigned int* err,
-                                          const SmallSide& S)
+                                          const SmallSide& S, int* __restrict__ lbase)
 {
     const int c0 = C - 1;
     const int ic = c0 % g.ncx + 1, jc = (c0 / g.ncx) % g.ncy + 1, kc = c0 / (g.ncx * g.ncy) + 1;
@@ -412,16 +414,14 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
     unsigned lt_mask;  // lanes below this one
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt_mask));
     float4 fi[Q];
-    int k[Q], ks[Q], cs[Q];
+    int k[Q], ks[Q];
 #pragma unroll
     for (int q = 0; q < Q; q++) {
         k[q] = 0;
         ks[q] = 0;
-        cs[q] = 0;
         if (q >= nq) continue;
         const double4 pi = P4[i0 + q];
         fi[q] = P4f[i0 + q];
-        if (BOTH) cs[q] = S.cell[i0 + q];
         const double lox = pi.x - (g.xmin + (ic - 1) * g.re) - mx;
         const double hix = (g.xmin + ic * g.re) - pi.x - mx;
         const double loy = pi.y - (g.ymin + (jc - 1) * g.re) - mx;
@@ -445,7 +445,7 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
         }
     }
     // one batch of 32 candidates against the Q particles
-    auto batch = [&](int j, bool valid, float4 fj) {
+    auto batch = [&](int j, bool valid, float4 fj, unsigned tag) {
 #pragma unroll
         for (int q = 0; q < Q; q++) {
             if (q >= nq) break;
@@ -469,7 +469,7 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
             if (m) {  // warp-uniform: many batches hold no member of this particle
                 if (in) {
                     const int pos = k[q] + __popc(m & lt_mask);
-                    if (pos < cap) out[(size_t)i * cap + pos] = j;
+                    if (pos < cap) out[(size_t)i * cap + pos] = (int)((unsigned)j | tag);
                 }
                 k[q] += __popc(m);
                 if (BOTH) {
@@ -485,7 +485,7 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
                                                          DIM == 3 ? pj.z - pi.z : 0.0);
                             ins = (DIM == 3) ? (d2 <= S.cut) : (d2 < S.cut);
                         }
-                        if (ins) ins = pnd_cells_adjacent(S, cs[q], S.cell[j]);
+                        if (ins) ins = pnd_cells_adjacent(fi[q].w, fj.w);
                     }
                     const unsigned ms = __ballot_sync(0xffffffffu, ins);
                     if (ms) {
@@ -499,11 +499,11 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
             }
         }
     };
-    auto scan = [&](int b, int e) {
+    auto scan = [&](int b, int e, unsigned tag) {
         for (int base = b; base < e; base += 32) {
             const int j = base + lane;
             const bool valid = j < e;
-            batch(j, valid, valid ? P4f[j] : make_float4(0.f, 0.f, 0.f, 0.f));
+            batch(j, valid, valid ? P4f[j] : make_float4(0.f, 0.f, 0.f, 0.f), tag);
         }
     };
     // the candidate range of every scanned (y, z) run, loaded at once (lane t
@@ -518,9 +518,14 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
         rb = cst[Cr + rlo];
         rend = cst[Cr + rhi] + cnt[Cr + rhi];
     }
+    // entries carry their run t (bits 28-31) and each row the runs' first
+    // slots, against which the PPE matrix codes its columns
+    if (lbase && lane < nt)
+        for (int q = 0; q < nq; q++) lbase[(size_t)(i0 + q) * kLapRuns + lane] = rb;
     for (int t = 0; t < nt; t++) {
         if (!(scan_t >> t & 1u)) continue;
-        scan(__shfl_sync(0xffffffffu, rb, t), __shfl_sync(0xffffffffu, rend, t));
+        scan(__shfl_sync(0xffffffffu, rb, t), __shfl_sync(0xffffffffu, rend, t),
+             lbase ? (unsigned)t << kSlotBits : 0u);
     }
     if (lane == 0) {
 #pragma unroll
@@ -554,7 +559,7 @@ __global__ void __launch_bounds__(256, 4) k_lists_q(int n, Grid g, double cut, f
                           const int* __restrict__ cell, const int* __restrict__ cst,
                           const int* __restrict__ cnt, int* __restrict__ out,
                           int* __restrict__ len, int* len_max, int which, unsigned int* err,
-                          SmallSide S)
+                          SmallSide S, int* __restrict__ lbase)
 {
     const int lane = threadIdx.x & 31;
     const long w = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -566,11 +571,11 @@ __global__ void __launch_bounds__(256, 4) k_lists_q(int n, Grid g, double cut, f
     for (int q = 1; q < nq; q++) same = same && cell[i0 + q] == C;
     if (same) {
         list_rows<DIM, Q, BOTH>(lane, i0, nq, C, g, cut, cut_lo, cut_hi, cap, P4, P4f, cst, cnt,
-                                out, len, len_max, which, err, S);
+                                out, len, len_max, which, err, S, lbase);
     } else {
         for (int q = 0; q < nq; q++)
             list_rows<DIM, Q, BOTH>(lane, i0 + q, 1, cell[i0 + q], g, cut, cut_lo, cut_hi, cap, P4,
-                                    P4f, cst, cnt, out, len, len_max, which, err, S);
+                                    P4f, cst, cnt, out, len, len_max, which, err, S, lbase);
     }
 }
 
@@ -710,12 +715,12 @@ int vmps_neighbors(mps_ctx* ctx)
         auto lo = [&](double c) { return std::nextafter((float)(c - ctx->screen_abs), 0.f); };
         auto hi = [&](double c) { return std::nextafter((float)(c + ctx->screen_abs), INFINITY); };
         float lo_l = lo(ctx->cut_l), hi_l = hi(ctx->cut_l), lo_s = lo(ctx->cut_s), hi_s = hi(ctx->cut_s);
-        SmallSide S{ctx->cut_s, lo_s,          hi_s,          ctx->cap_s, ctx->nbr_s,
-                    ctx->len_s, ctx->cell_s,   ctx->gs.ncx,   ctx->gs.ncx * ctx->gs.ncy};
+        SmallSide S{ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->nbr_s, ctx->len_s};
 #define LISTS_Q(D, B)                                                                          \
     k_lists_q<D, kListQ, B><<<nq32, kBlock, 0, st>>>(                                          \
         n, ctx->gl, ctx->cut_l, lo_l, hi_l, ctx->cap_l, ctx->P4, ctx->P4f, ctx->cell_l,        \
-        ctx->cst_l, ctx->cnt_l, ctx->nbr_l, ctx->len_l, ctx->len_max, 0, ctx->d_err, S)
+        ctx->cst_l, ctx->cnt_l, ctx->nbr_l, ctx->len_l, ctx->len_max, 0, ctx->d_err, S,     \
+        ctx->lbase)
 #define LISTS_S(D, G)                                                                          \
     k_lists<D, G><<<(int)(((long)n * G + kBlock - 1) / kBlock), kBlock, 0, st>>>(               \
         n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,         \
