@@ -138,25 +138,25 @@ class ClockSampler:
 
 
 def spmv_algorithmic_bytes(nnz_a: float, rows: float) -> float:
-    """Bytes one FP64 SpMV must move: per stored non-zero a 16-bit column code
-    (2 B) and a value (8 B); per unknown row its (offset, length) pair (8), its
-    nine run bases (36), diag (8), the row's own p (8) and the written s (8).
+    """Bytes one FP64 CSR SpMV must move: per stored non-zero a column index
+    (4 B) and a value (8 B); per unknown row its (offset, length) pair (8),
+    diag (8), the row's own p (8) and the written s (8), and bcon (4).
     Gathers of p_j are L2 hits."""
-    return nnz_a * 10.0 + rows * 68.0
+    return nnz_a * 12.0 + rows * 36.0
 
 
 def spmv32_algorithmic_bytes(nnz_a: float, rows: float) -> float:
     """Inner SpMV of the mixed-precision PPE: one (column, FP32 value) pair
     (8 B) per non-zero; per row (offset, length) (8), diag (8), FP32 p and s
-    (4 each)."""
-    return nnz_a * 8.0 + rows * 24.0
+    (4 each), bcon (4)."""
+    return nnz_a * 8.0 + rows * 28.0
 
 
 def refine_algorithmic_bytes(nnz_a: float, rows: float) -> float:
-    """Refinement r -= A64 d, x += d: 10 B per non-zero as the FP64 SpMV; per
-    row (offset, length) (8), run bases (36), diag (8), FP32 d (4), r and x
-    read and written (32)."""
-    return nnz_a * 10.0 + rows * 88.0
+    """Refinement r -= A64 d, x += d: 12 B per non-zero; per row (offset,
+    length) (8), diag (8), bcon, FP32 d (4 each), r and x read and written
+    (32)."""
+    return nnz_a * 12.0 + rows * 56.0
 
 
 WORKLOADS = {

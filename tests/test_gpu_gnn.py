@@ -23,6 +23,9 @@ Y_TOL = 1e-2
 # gradient: FP32 sums in a different order than the FP64 oracle, on the
 # tensor-core forward's activations
 GRAD_TOL = 1e-2
+# the trained guess must leave at most this fraction of the previous
+# pressure's starting residual |b - A x0| / |b|
+GAIN_R0 = 0.5
 
 
 def _ctx(steps=2, seed=7, scale=0.1):
@@ -143,6 +146,10 @@ def test_learned_guess_keeps_the_answer_and_reports_iterations():
     print(f"\nprevious-pressure guess: |r0|/|b| {np.mean(r0_b):.3g}, CG iterations "
           f"{np.mean(its_b):.2f}; learned guess: |r0|/|b| {np.mean(r0_g):.3g}, "
           f"CG iterations {np.mean(its_g):.2f}")
+    # what the trained network gains: a smaller starting residual than the
+    # previous pressure leaves, and no more CG iterations
+    assert np.mean(r0_g) <= GAIN_R0 * np.mean(r0_b)
+    assert np.mean(its_g) <= np.mean(its_b)
     base.close()
     s.close()
 

@@ -243,8 +243,7 @@ int allocate(mps_ctx* c)
     TRY(dalloc(c, &c->nbr_l, (size_t)c->cap_l * P));
     TRY(dalloc(c, &c->nbr_s, (size_t)c->cap_s * P));
     TRY(dalloc(c, &c->mrow, P));
-    TRY(dalloc(c, &c->lbase, (size_t)kLapRuns * P));
-    TRY(dalloc(c, &c->mcode, (size_t)c->cap_l * P));
+    TRY(dalloc(c, &c->mcol, (size_t)c->cap_l * P));
     TRY(dalloc(c, &c->mval, (size_t)c->cap_l * P));
     if (c->cfg.precision == 1) {
         TRY(dalloc(c, &c->mcv32, (size_t)c->cap_l * P));
@@ -348,10 +347,6 @@ int mps_upload(mps_ctx* c, int n, const double* x, const double* y, const double
                const double* p)
 {
     if (!c || n <= 0 || !x || !y || !ptype || (c->cfg.dim == 3 && !z)) return MPS_ERR_ARG;
-    if ((unsigned)n > kSlotMask) {  // list entries carry the slot in 28 bits
-        c->msg = "at most 2^28 - 1 particles per context";
-        return MPS_ERR_ARG;
-    }
     VMPS_CUDA(c, cudaSetDevice(c->device));
     free_all(c);
     vmps_gnn_reset(c);
@@ -404,12 +399,6 @@ int mps_upload(mps_ctx* c, int n, const double* x, const double* y, const double
     bool strict = f.dim == 2;
     c->cut_l = sqrt_cut(strict ? f.re_l : f.re_l + f.delta, strict);
     c->cut_s = sqrt_cut(strict ? f.re_s : f.re_s + f.delta, strict);
-    // the PND-radius list can be taken from the Laplacian pass when its
-    // cutoff lies well inside the Laplacian cells (then every PND neighbour
-    // is a Laplacian neighbour): 2.1 against 4.0 l0 in every benchmark case
-    c->fuse_lists = (strict ? f.re_s : f.re_s + f.delta) <= 0.9 * f.re_l && c->gs.ncx <= 1024 &&
-                    c->gs.ncy <= 1024 && c->gs.ncz <= 1024;
-    c->perm_s_valid = false;
     c->cap_l = f.list_cap_l > 0 ? (f.list_cap_l + 7) / 8 * 8 : auto_cap(f, f.re_l);
     c->cap_s = f.list_cap_s > 0 ? (f.list_cap_s + 7) / 8 * 8 : auto_cap(f, f.re_s);
     c->lambda_l = 0.0;  // main.cu:491-494 at the Laplacian radius
@@ -891,7 +880,6 @@ int mps_download(mps_ctx* c, const char* field, void* out, long* count)
         k_unpermute_i<<<grid_blocks(n), kBlock, 0, st>>>(n, c->oid, a, istage);
         VMPS_CUDA(c, cudaMemcpyAsync(out, istage, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
     } else if (f == "perm_l" || f == "perm_s") {
-        if (f == "perm_s") TRY(vmps_perm_s(c));
         k_perm_ids<<<grid_blocks(n), kBlock, 0, st>>>(n, c->oid, f == "perm_s" ? c->perm_s : nullptr,
                                                        istage);
         VMPS_CUDA(c, cudaMemcpyAsync(out, istage, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
@@ -943,7 +931,7 @@ int mps_download_lists(mps_ctx* c, int which, int* off, int* nbr, long* total)
             coords(cell[i], ai, bi, ki);
             keyed.clear();
             for (int k = 0; k < len[i]; k++) {
-                int j = (int)((unsigned)ent[(size_t)i * cap + k] & kSlotMask);
+                int j = ent[(size_t)i * cap + k];
                 int aj, bj, kj;
                 coords(cell[j], aj, bj, kj);
                 long rank = (long)(aj - ai + 1) * 9 + (bj - bi + 1) * 3 + (kj - ki + 1);

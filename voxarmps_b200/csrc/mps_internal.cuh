@@ -198,18 +198,10 @@ struct mps_ctx {
     int *bslot_s = nullptr, *boid_s = nullptr;
     int *src = nullptr, *inv = nullptr;            // new slot <- old slot, old -> new
     int *perm_s = nullptr, *perm_s_tmp = nullptr;  // small-grid cell order (slots)
-    // the PND-radius list is derived in the Laplacian list's pass (its
-    // support lies well inside the Laplacian radius); the PND grid's sort
-    // order is then only formed when it is downloaded
-    bool fuse_lists = false;
-    bool perm_s_valid = false;
     // lists (slot-major)
     int *nbr_l = nullptr, *len_l = nullptr, *nbr_s = nullptr, *len_s = nullptr;
-    int* lbase = nullptr;  // first slot of each run of a Laplacian row (kLapRuns per row)
-    // PPE matrix (compact slot-major CSR: row i at moff[i]) and CG vectors;
-    // columns as 16-bit (run, offset) codes against lbase
-    unsigned short* mcode = nullptr;
-    int *mlen = nullptr, *moff = nullptr;
+    // PPE matrix (compact slot-major ELL) and CG vectors
+    int *mcol = nullptr, *mlen = nullptr, *moff = nullptr;  // CSR: row i at moff[i]
     int2* mrow = nullptr;  // (moff, mlen) per row, mlen -1 for rows outside the system
     double* mval = nullptr;
     double *pres_x = nullptr, *pres_y = nullptr, *pres_z = nullptr;  // prediction pressure sums
@@ -330,29 +322,6 @@ __device__ __forceinline__ bool cell_coords(const Grid& g, double x, double y, d
 
 inline int grid_blocks(long n) { return (int)((n + kBlock - 1) / kBlock); }
 
-// Laplacian-list entries: bits 0-27 the neighbour's slot, bits 28-31 the
-// run of cells (one (y, z) offset's x-triple, kLapRuns per row) in which the
-// list pass found it; kLapRuns first slots per row (lbase) go with them.  The
-// PPE matrix codes each column as (run, slot - first slot of the run) in 16
-// bits.
-constexpr int kSlotBits = 28;
-constexpr unsigned kSlotMask = (1u << kSlotBits) - 1u;
-constexpr int kLapRuns = 9;
-constexpr int kRunOffBits = 12;
-constexpr unsigned kRunOffMask = (1u << kRunOffBits) - 1u;
-
-// The w slot of the FP32 positions (P4f): bits 0-1 the particle kind + 1
-// (PTYPE -1..2), bits 2-11, 12-21, 22-31 the 0-based x, y, z cell of the
-// particle on the PND grid (each axis at most 1024 cells when it is used).
-__host__ __device__ __forceinline__ unsigned pnd_cell_word(int ptype, int cell, int ncx, int ncxy)
-{
-    const int c = cell - 1;
-    const unsigned a = (unsigned)(c % ncx), b = (unsigned)((c % ncxy) / ncx),
-                   k = (unsigned)(c / ncxy);
-    return (unsigned)(ptype + 1) | ((a & 1023u) << 2) | ((b & 1023u) << 12) | ((k & 1023u) << 22);
-}
-__device__ __forceinline__ int pnd_word_ptype(float w) { return (int)(__float_as_uint(w) & 3u) - 1; }
-
 // W() of functions.cu:32-74 from d2 and rD = rsqrt(d2)
 template <int DIM>
 __device__ __forceinline__ double w_fast(const WK& k, double d2, double rD)
@@ -395,7 +364,7 @@ template <int DIM>
 __device__ __forceinline__ float w_fast32(const WKf& k, float d2)
 {
     const float rD = rsqrtf(d2);
-    if (k.ktype == 2) return d2 < k.lt ? k.re * rD - 1.f : 0.f;
+    if (k.ktype == 2) return d2 < k.lt ? __fmaf_rn(k.re, rD, -1.f) : 0.f;
     const float R = d2 * rD, q = R * k.inv_re;
     switch (k.ktype) {
     case 6:
@@ -478,7 +447,6 @@ int vmps_check(mps_ctx* ctx, cudaError_t e, const char* what);
 
 // stage launchers (defined in the kernel translation units)
 int vmps_neighbors(mps_ctx* ctx);
-int vmps_perm_s(mps_ctx* ctx);  // PND-grid order, formed on demand
 int vmps_pnd(mps_ctx* ctx, int at_star, int correct, int which_list, double* out);
 int vmps_max_reduce(mps_ctx* ctx, const double* a, double* result);
 int vmps_sps(mps_ctx* ctx);

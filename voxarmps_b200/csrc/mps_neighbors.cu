@@ -24,9 +24,7 @@ using namespace vmps;
 
 namespace {
 
-// COUNT_S: also bucket-count the PND grid (its sort order is formed in the
-// same pass); without it only its cell numbers are kept
-template <int DIM, bool COUNT_S>
+template <int DIM>
 __global__ void k_hash(int n, Grid gl, Grid gs, const double* __restrict__ x,
                        const double* __restrict__ y, const double* __restrict__ z,
                        int* __restrict__ cell_l, int* __restrict__ cell_s,
@@ -45,15 +43,7 @@ __global__ void k_hash(int n, Grid gl, Grid gs, const double* __restrict__ x,
     cell_l[i] = Cl;
     cell_s[i] = Cs;
     bpos_l[i] = atomicAdd(&cnt_l[Cl], 1);
-    if (COUNT_S) bpos_s[i] = atomicAdd(&cnt_s[Cs], 1);
-}
-
-// bucket counts of one grid from stored cell numbers
-__global__ void k_count(int n, const int* __restrict__ cell, int* __restrict__ cnt,
-                        int* __restrict__ bpos)
-{
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) bpos[i] = atomicAdd(&cnt[cell[i]], 1);
+    bpos_s[i] = atomicAdd(&cnt_s[Cs], 1);
 }
 
 // three-phase exclusive scan (tile sums, scan of tile sums, tile rescans)
@@ -149,35 +139,6 @@ __global__ void k_scatter(int n, const int* __restrict__ cell_l, const int* __re
     int qs = cst_s[cell_s[i]] + bpos_s[i];
     bslot_s[qs] = i;
     boid_s[qs] = o;
-}
-
-// one grid: particles into their cell bucket
-__global__ void k_scatter1(int n, const int* __restrict__ cell, const int* __restrict__ bpos,
-                           const int* __restrict__ cst, const int* __restrict__ oid,
-                           int* __restrict__ bslot, int* __restrict__ boid)
-{
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int q = cst[cell[i]] + bpos[i];
-    bslot[q] = i;
-    boid[q] = oid[i];
-}
-
-// one grid: rank inside the bucket by original id; sorted[new] = slot and,
-// when inv is given, inv[slot] = new
-__global__ void k_rank1(int n, const int* __restrict__ cell, const int* __restrict__ cst,
-                        const int* __restrict__ cnt, const int* __restrict__ bslot,
-                        const int* __restrict__ boid, int* __restrict__ sorted,
-                        int* __restrict__ inv)
-{
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= n) return;
-    int s = bslot[q], me = boid[q];
-    int c = cell[s];
-    int b = cst[c], e = b + cnt[c], r = 0;
-    for (int t = b; t < e; t++) r += (boid[t] < me);
-    sorted[b + r] = s;
-    if (inv) inv[s] = b + r;
 }
 
 // Rank inside the bucket by original id.  Primary grid: src[new] = old slot
@@ -351,33 +312,6 @@ __global__ void __launch_bounds__(256, 8) k_lists(int n, Grid g, double cut, flo
     }
 }
 
-// The PND-radius list taken in the Laplacian list's pass: a Laplacian
-// neighbour j of i is a PND neighbour when it passes NEIGHBOR's distance rule
-// at the PND cutoff and sits in one of the 3x3(x3) PND-grid cells around i's
-// (functions.cu:2854-2918 on the PND grid; in 3D that cell rule is not implied
-// by the distance, x/y cells being re wide under a cutoff of re + DELTA).
-// The cell test reads the PND-grid cells packed with the positions, so it
-// adds no load to the candidate loop.
-struct SmallSide {
-    double cut;         // squared-distance threshold (3D <=, 2D <)
-    float lo, hi;       // FP32 screening window around cut
-    int cap;            // row capacity
-    int* out;           // rows, i * cap
-    int* len;           // row lengths
-};
-
-// PND-grid cells of two particles within one cell of each other along every
-// axis; the cells come packed in the w slot of their FP32 positions
-// (pnd_cell_word)
-__device__ __forceinline__ bool pnd_cells_adjacent(float wi, float wj)
-{
-    const unsigned a = __float_as_uint(wi), b = __float_as_uint(wj);
-    const int dx = (int)((a >> 2) & 1023u) - (int)((b >> 2) & 1023u);
-    const int dy = (int)((a >> 12) & 1023u) - (int)((b >> 12) & 1023u);
-    const int dz = (int)(a >> 22) - (int)(b >> 22);
-    return abs(dx) <= 1 && abs(dy) <= 1 && abs(dz) <= 1;
-}
-
 // The same lists for Q particles of one cell at a time, one warp: each
 // candidate's packed position is loaded once and tested against the Q
 // particles, so the load, the loop and the index work are shared.  The
@@ -385,17 +319,15 @@ __device__ __forceinline__ bool pnd_cells_adjacent(float wi, float wj)
 // a particle would have culled holds none of its neighbours, so every row
 // receives exactly the entries, in exactly the order, of the one-particle
 // kernel above.  Groups whose particles sit in different cells are done
-// one particle at a time.  BOTH: the PND-radius rows as well (SmallSide),
-// in the same scan order.
-template <int DIM, int Q, bool BOTH>
+// one particle at a time.
+template <int DIM, int Q>
 __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const Grid& g,
                                           double cut, float cut_lo, float cut_hi, int cap,
                                           const double4* __restrict__ P4,
                                           const float4* __restrict__ P4f,
                                           const int* __restrict__ cst, const int* __restrict__ cnt,
                                           int* __restrict__ out, int* __restrict__ len,
-                                          int* len_max, int which, unsigned int* err,
-                                          const SmallSide& S, int* __restrict__ lbase)
+                                          int* len_max, int which, unsigned int* err)
 {
     const int c0 = C - 1;
     const int ic = c0 % g.ncx + 1, jc = (c0 / g.ncx) % g.ncy + 1, kc = c0 / (g.ncx * g.ncy) + 1;
@@ -414,11 +346,10 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
     unsigned lt_mask;  // lanes below this one
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt_mask));
     float4 fi[Q];
-    int k[Q], ks[Q];
+    int k[Q];
 #pragma unroll
     for (int q = 0; q < Q; q++) {
         k[q] = 0;
-        ks[q] = 0;
         if (q >= nq) continue;
         const double4 pi = P4[i0 + q];
         fi[q] = P4f[i0 + q];
@@ -445,17 +376,16 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
         }
     }
     // one batch of 32 candidates against the Q particles
-    auto batch = [&](int j, bool valid, float4 fj, unsigned tag) {
+    auto batch = [&](int j, bool valid, float4 fj) {
 #pragma unroll
         for (int q = 0; q < Q; q++) {
             if (q >= nq) break;
             const int i = i0 + q;
             bool in = false;
-            float f2 = 0.f;
             if (valid) {
                 const float ex = fj.x - fi[q].x, ey = fj.y - fi[q].y,
                             ez = DIM == 3 ? fj.z - fi[q].z : 0.f;
-                f2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
+                const float f2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
                 if (f2 < cut_lo) {
                     in = (DIM == 3) || (j != i);
                 } else if (f2 <= cut_hi) {
@@ -469,41 +399,17 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
             if (m) {  // warp-uniform: many batches hold no member of this particle
                 if (in) {
                     const int pos = k[q] + __popc(m & lt_mask);
-                    if (pos < cap) out[(size_t)i * cap + pos] = (int)((unsigned)j | tag);
+                    if (pos < cap) out[(size_t)i * cap + pos] = j;
                 }
                 k[q] += __popc(m);
-                if (BOTH) {
-                    // PND rule: exact distance inside the screening window,
-                    // then the PND-grid cell rule
-                    bool ins = false;
-                    if (in) {
-                        if (f2 < S.lo) {
-                            ins = true;
-                        } else if (f2 <= S.hi) {
-                            const double4 pi = P4[i], pj = P4[j];
-                            const double d2 = dist2<DIM>(pj.x - pi.x, pj.y - pi.y,
-                                                         DIM == 3 ? pj.z - pi.z : 0.0);
-                            ins = (DIM == 3) ? (d2 <= S.cut) : (d2 < S.cut);
-                        }
-                        if (ins) ins = pnd_cells_adjacent(fi[q].w, fj.w);
-                    }
-                    const unsigned ms = __ballot_sync(0xffffffffu, ins);
-                    if (ms) {
-                        if (ins) {
-                            const int pos = ks[q] + __popc(ms & lt_mask);
-                            if (pos < S.cap) S.out[(size_t)i * S.cap + pos] = j;
-                        }
-                        ks[q] += __popc(ms);
-                    }
-                }
             }
         }
     };
-    auto scan = [&](int b, int e, unsigned tag) {
+    auto scan = [&](int b, int e) {
         for (int base = b; base < e; base += 32) {
             const int j = base + lane;
             const bool valid = j < e;
-            batch(j, valid, valid ? P4f[j] : make_float4(0.f, 0.f, 0.f, 0.f), tag);
+            batch(j, valid, valid ? P4f[j] : make_float4(0.f, 0.f, 0.f, 0.f));
         }
     };
     // the candidate range of every scanned (y, z) run, loaded at once (lane t
@@ -518,14 +424,9 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
         rb = cst[Cr + rlo];
         rend = cst[Cr + rhi] + cnt[Cr + rhi];
     }
-    // entries carry their run t (bits 28-31) and each row the runs' first
-    // slots, against which the PPE matrix codes its columns
-    if (lbase && lane < nt)
-        for (int q = 0; q < nq; q++) lbase[(size_t)(i0 + q) * kLapRuns + lane] = rb;
     for (int t = 0; t < nt; t++) {
         if (!(scan_t >> t & 1u)) continue;
-        scan(__shfl_sync(0xffffffffu, rb, t), __shfl_sync(0xffffffffu, rend, t),
-             lbase ? (unsigned)t << kSlotBits : 0u);
+        scan(__shfl_sync(0xffffffffu, rb, t), __shfl_sync(0xffffffffu, rend, t));
     }
     if (lane == 0) {
 #pragma unroll
@@ -538,28 +439,18 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
                 kq = cap;
             }
             len[i0 + q] = kq;
-            if (BOTH) {
-                int kp = ks[q];
-                atomicMax(&len_max[1], kp);
-                if (kp > S.cap) {
-                    set_error(err, MPS_ERR_LIST_OVERFLOW);
-                    kp = S.cap;
-                }
-                S.len[i0 + q] = kp;
-            }
         }
     }
 }
 
 // 4 resident blocks per SM (at most 64 registers; 66 without the bound
 // would leave 3)
-template <int DIM, int Q, bool BOTH>
+template <int DIM, int Q>
 __global__ void __launch_bounds__(256, 4) k_lists_q(int n, Grid g, double cut, float cut_lo, float cut_hi, int cap,
                           const double4* __restrict__ P4, const float4* __restrict__ P4f,
                           const int* __restrict__ cell, const int* __restrict__ cst,
                           const int* __restrict__ cnt, int* __restrict__ out,
-                          int* __restrict__ len, int* len_max, int which, unsigned int* err,
-                          SmallSide S, int* __restrict__ lbase)
+                          int* __restrict__ len, int* len_max, int which, unsigned int* err)
 {
     const int lane = threadIdx.x & 31;
     const long w = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -570,12 +461,12 @@ __global__ void __launch_bounds__(256, 4) k_lists_q(int n, Grid g, double cut, f
     bool same = true;
     for (int q = 1; q < nq; q++) same = same && cell[i0 + q] == C;
     if (same) {
-        list_rows<DIM, Q, BOTH>(lane, i0, nq, C, g, cut, cut_lo, cut_hi, cap, P4, P4f, cst, cnt,
-                                out, len, len_max, which, err, S, lbase);
+        list_rows<DIM, Q>(lane, i0, nq, C, g, cut, cut_lo, cut_hi, cap, P4, P4f, cst, cnt, out,
+                          len, len_max, which, err);
     } else {
         for (int q = 0; q < nq; q++)
-            list_rows<DIM, Q, BOTH>(lane, i0 + q, 1, cell[i0 + q], g, cut, cut_lo, cut_hi, cap, P4,
-                                    P4f, cst, cnt, out, len, len_max, which, err, S, lbase);
+            list_rows<DIM, Q>(lane, i0 + q, 1, cell[i0 + q], g, cut, cut_lo, cut_hi, cap, P4, P4f,
+                              cst, cnt, out, len, len_max, which, err);
     }
 }
 
@@ -651,38 +542,26 @@ int vmps_neighbors(mps_ctx* ctx)
     const int n = ctx->n;
     cudaStream_t st = ctx->stream;
     int nb = grid_blocks(n);
-    const bool fused = ctx->fuse_lists;
     VMPS_CUDA(ctx, cudaMemsetAsync(ctx->cnt_l, 0, sizeof(int) * (ctx->gl.tnc + 2), st));
-    if (!fused) VMPS_CUDA(ctx, cudaMemsetAsync(ctx->cnt_s, 0, sizeof(int) * (ctx->gs.tnc + 2), st));
+    VMPS_CUDA(ctx, cudaMemsetAsync(ctx->cnt_s, 0, sizeof(int) * (ctx->gs.tnc + 2), st));
     VMPS_CUDA(ctx, cudaMemsetAsync(ctx->len_max, 0, sizeof(int) * 2, st));
-#define HASH(D, CS)                                                                              \
-    k_hash<D, CS><<<nb, kBlock, 0, st>>>(n, ctx->gl, ctx->gs, ctx->x, ctx->y, ctx->z, ctx->cell_l, \
-                                         ctx->cell_s, ctx->cnt_l, ctx->cnt_s, ctx->bpos_l,         \
-                                         ctx->bpos_s, ctx->d_err)
-    if (ctx->cfg.dim == 3) {
-        if (fused) HASH(3, false); else HASH(3, true);
-    } else {
-        if (fused) HASH(2, false); else HASH(2, true);
-    }
-#undef HASH
+    if (ctx->cfg.dim == 3)
+        k_hash<3><<<nb, kBlock, 0, st>>>(n, ctx->gl, ctx->gs, ctx->x, ctx->y, ctx->z, ctx->cell_l,
+                                         ctx->cell_s, ctx->cnt_l, ctx->cnt_s, ctx->bpos_l,
+                                         ctx->bpos_s, ctx->d_err);
+    else
+        k_hash<2><<<nb, kBlock, 0, st>>>(n, ctx->gl, ctx->gs, ctx->x, ctx->y, ctx->z, ctx->cell_l,
+                                         ctx->cell_s, ctx->cnt_l, ctx->cnt_s, ctx->bpos_l,
+                                         ctx->bpos_s, ctx->d_err);
     vmps_count_launch(1);
     scan(ctx, ctx->gl.tnc + 2, ctx->cnt_l, ctx->cst_l, ctx->scan_tmp);
-    if (fused) {
-        // the Laplacian grid's order only; the PND grid's is formed on demand
-        k_scatter1<<<nb, kBlock, 0, st>>>(n, ctx->cell_l, ctx->bpos_l, ctx->cst_l, ctx->oid,
-                                          ctx->bslot_l, ctx->boid_l);
-        k_rank1<<<nb, kBlock, 0, st>>>(n, ctx->cell_l, ctx->cst_l, ctx->cnt_l, ctx->bslot_l,
-                                       ctx->boid_l, ctx->src, ctx->inv);
-    } else {
-        scan(ctx, ctx->gs.tnc + 2, ctx->cnt_s, ctx->cst_s, ctx->scan_tmp);
-        k_scatter<<<nb, kBlock, 0, st>>>(n, ctx->cell_l, ctx->cell_s, ctx->bpos_l, ctx->bpos_s,
-                                         ctx->cst_l, ctx->cst_s, ctx->oid, ctx->bslot_l,
-                                         ctx->boid_l, ctx->bslot_s, ctx->boid_s);
-        k_rank<<<nb, kBlock, 0, st>>>(n, ctx->cell_l, ctx->cell_s, ctx->cst_l, ctx->cnt_l,
-                                      ctx->cst_s, ctx->cnt_s, ctx->bslot_l, ctx->boid_l,
-                                      ctx->bslot_s, ctx->boid_s, ctx->src, ctx->inv,
-                                      ctx->perm_s_tmp);
-    }
+    scan(ctx, ctx->gs.tnc + 2, ctx->cnt_s, ctx->cst_s, ctx->scan_tmp);
+    k_scatter<<<nb, kBlock, 0, st>>>(n, ctx->cell_l, ctx->cell_s, ctx->bpos_l, ctx->bpos_s,
+                                     ctx->cst_l, ctx->cst_s, ctx->oid, ctx->bslot_l, ctx->boid_l,
+                                     ctx->bslot_s, ctx->boid_s);
+    k_rank<<<nb, kBlock, 0, st>>>(n, ctx->cell_l, ctx->cell_s, ctx->cst_l, ctx->cnt_l, ctx->cst_s,
+                                  ctx->cnt_s, ctx->bslot_l, ctx->boid_l, ctx->bslot_s,
+                                  ctx->boid_s, ctx->src, ctx->inv, ctx->perm_s_tmp);
     vmps_count_launch(2);
     // reorder persistent state into cell order
     GatherSet g;
@@ -692,11 +571,8 @@ int vmps_neighbors(mps_ctx* ctx)
     k_gather<<<nb, kBlock, 0, st>>>(n, ctx->src, g);
     vmps_count_launch(1);
     vmps_reorder_swap(ctx);
-    if (!fused) {
-        k_translate<<<nb, kBlock, 0, st>>>(n, ctx->inv, ctx->perm_s_tmp, ctx->perm_s);
-        vmps_count_launch(1);
-    }
-    ctx->perm_s_valid = !fused;
+    k_translate<<<nb, kBlock, 0, st>>>(n, ctx->inv, ctx->perm_s_tmp, ctx->perm_s);
+    vmps_count_launch(1);
     if (ctx->nscenes > 1) {
         k_scene_ranges_init<<<grid_blocks(ctx->nscenes), kBlock, 0, st>>>(ctx->nscenes, n,
                                                                           ctx->sfirst, ctx->slast);
@@ -715,42 +591,39 @@ int vmps_neighbors(mps_ctx* ctx)
         auto lo = [&](double c) { return std::nextafter((float)(c - ctx->screen_abs), 0.f); };
         auto hi = [&](double c) { return std::nextafter((float)(c + ctx->screen_abs), INFINITY); };
         float lo_l = lo(ctx->cut_l), hi_l = hi(ctx->cut_l), lo_s = lo(ctx->cut_s), hi_s = hi(ctx->cut_s);
-        SmallSide S{ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->nbr_s, ctx->len_s};
-#define LISTS_Q(D, B)                                                                          \
-    k_lists_q<D, kListQ, B><<<nq32, kBlock, 0, st>>>(                                          \
-        n, ctx->gl, ctx->cut_l, lo_l, hi_l, ctx->cap_l, ctx->P4, ctx->P4f, ctx->cell_l,        \
-        ctx->cst_l, ctx->cnt_l, ctx->nbr_l, ctx->len_l, ctx->len_max, 0, ctx->d_err, S,     \
-        ctx->lbase)
-#define LISTS_S(D, G)                                                                          \
-    k_lists<D, G><<<(int)(((long)n * G + kBlock - 1) / kBlock), kBlock, 0, st>>>(               \
-        n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,         \
-        ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1, ctx->d_err)
         if (ctx->cfg.dim == 3) {
             constexpr int GS = SmallG<3>::G;
-            if (fused) {
-                LISTS_Q(3, true);
-                vmps_count_launch(1);
-            } else {
-                LISTS_Q(3, false);
-                if (ctx->tune_small_wide) LISTS_S(3, 2 * GS);
-                else LISTS_S(3, GS);
-                vmps_count_launch(2);
-            }
+            k_lists_q<3, kListQ><<<nq32, kBlock, 0, st>>>(
+                n, ctx->gl, ctx->cut_l, lo_l, hi_l, ctx->cap_l, ctx->P4, ctx->P4f, ctx->cell_l,
+                ctx->cst_l, ctx->cnt_l, ctx->nbr_l, ctx->len_l, ctx->len_max, 0, ctx->d_err);
+            if (ctx->tune_small_wide)
+                k_lists<3, 2 * GS><<<(int)(((long)n * 2 * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+                    n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,
+                    ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
+                    ctx->d_err);
+            else
+                k_lists<3, GS><<<(int)(((long)n * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+                    n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,
+                    ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
+                    ctx->d_err);
         } else {
             constexpr int GS = SmallG<2>::G;
-            if (fused) {
-                LISTS_Q(2, true);
-                vmps_count_launch(1);
-            } else {
-                LISTS_Q(2, false);
-                if (ctx->tune_small_wide) LISTS_S(2, 2 * GS);
-                else LISTS_S(2, GS);
-                vmps_count_launch(2);
-            }
+            k_lists_q<2, kListQ><<<nq32, kBlock, 0, st>>>(
+                n, ctx->gl, ctx->cut_l, lo_l, hi_l, ctx->cap_l, ctx->P4, ctx->P4f, ctx->cell_l,
+                ctx->cst_l, ctx->cnt_l, ctx->nbr_l, ctx->len_l, ctx->len_max, 0, ctx->d_err);
+            if (ctx->tune_small_wide)
+                k_lists<2, 2 * GS><<<(int)(((long)n * 2 * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+                    n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,
+                    ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
+                    ctx->d_err);
+            else
+                k_lists<2, GS><<<(int)(((long)n * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+                    n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,
+                    ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
+                    ctx->d_err);
         }
-#undef LISTS_Q
-#undef LISTS_S
     }
+    vmps_count_launch(2);
     if (ctx->profile) {
         VMPS_CUDA(ctx, cudaEventRecord(ctx->ev[7], st));
         VMPS_CUDA(ctx, cudaEventSynchronize(ctx->ev[7]));
@@ -760,27 +633,5 @@ int vmps_neighbors(mps_ctx* ctx)
         ctx->lists_launches++;
     }
     VMPS_CUDA(ctx, cudaGetLastError());
-    return MPS_OK;
-}
-
-// NEIGHBOR's permutation on the PND grid (ip[] of functions.cu:2820-2852)
-// for the current slots, when the last neighbour search did not form it:
-// stable counting sort of the slots by (PND cell, original id).
-int vmps_perm_s(mps_ctx* ctx)
-{
-    if (ctx->perm_s_valid) return MPS_OK;
-    const int n = ctx->n;
-    cudaStream_t st = ctx->stream;
-    const int nb = grid_blocks(n);
-    VMPS_CUDA(ctx, cudaMemsetAsync(ctx->cnt_s, 0, sizeof(int) * (ctx->gs.tnc + 2), st));
-    k_count<<<nb, kBlock, 0, st>>>(n, ctx->cell_s, ctx->cnt_s, ctx->bpos_s);
-    scan(ctx, ctx->gs.tnc + 2, ctx->cnt_s, ctx->cst_s, ctx->scan_tmp);
-    k_scatter1<<<nb, kBlock, 0, st>>>(n, ctx->cell_s, ctx->bpos_s, ctx->cst_s, ctx->oid,
-                                      ctx->bslot_s, ctx->boid_s);
-    k_rank1<<<nb, kBlock, 0, st>>>(n, ctx->cell_s, ctx->cst_s, ctx->cnt_s, ctx->bslot_s,
-                                   ctx->boid_s, ctx->perm_s, nullptr);
-    vmps_count_launch(3);
-    VMPS_CUDA(ctx, cudaGetLastError());
-    ctx->perm_s_valid = true;
     return MPS_OK;
 }

@@ -72,9 +72,6 @@ struct Asm {
 
 // one lane group (kAsmG lanes) per row; the non-zero columns are compacted in list order into
 // the row's CSR segment (capacity = the row's list length)
-// Columns are stored as 16-bit codes (run << 12 | slot - first slot of the
-// run) against the row's run bases from the list pass; an offset beyond 12
-// bits (a run holding over 4095 particles) is reported as a list overflow.
 template <int DIM>
 // 6 resident blocks per SM (40 registers, a few bytes of spills): measured
 // 0.2 ms per step faster than 5 on the 1.6 M-particle dam, 8 spills too much
@@ -82,11 +79,11 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
                            const int* __restrict__ len, const int* __restrict__ bcon,
                            const double4* __restrict__ P4, const double* __restrict__ nsrc,
                            int warm, double* __restrict__ pnew, double* __restrict__ pold,
-                           const int* __restrict__ moff, const int* __restrict__ lbase,
-                           unsigned short* __restrict__ mcode, double* __restrict__ mval,
+                           const int* __restrict__ moff,
+                           int* __restrict__ mcol, double* __restrict__ mval,
                            int2* __restrict__ mcv32, int* __restrict__ mlen,
                            double* __restrict__ diag, double* __restrict__ source, int w_bcon,
-                           int2* __restrict__ mrow, unsigned int* err)
+                           int2* __restrict__ mrow)
 {
     Grp<kAsmG> q;
     int i = (int)q.gid;
@@ -105,8 +102,7 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
     }
     double4 pi = P4[i];
     const int* row = nbr + (size_t)i * cap;
-    const int* rbase = lbase + (size_t)i * kLapRuns;
-    unsigned short* crow = mcode + moff[i];
+    int* crow = mcol + moff[i];
     double* vrow = mval + moff[i];
     double dg = 0.0;
     int cnt = 0, L = len[i];
@@ -114,12 +110,9 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
         int k = base + q.lane;
         double v = 0.0;
         int j = -1;
-        unsigned run = 0;
         bool keep = false;
         if (k < L) {
-            const unsigned e = (unsigned)row[k];
-            j = (int)(e & kSlotMask);
-            run = e >> kSlotBits;
+            j = row[k];
             double4 pj;
             int bj;
             if (w_bcon) {  // P4's w slot holds bcon: one gather
@@ -142,15 +135,8 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
         unsigned m = q.ballot(keep);
         if (keep) {
             int pos = cnt + __popc(m & ((1u << q.lane) - 1u));
-            unsigned off = (unsigned)(j - rbase[run]);
-            double val = -v;
-            if (off > kRunOffMask) {  // cannot be coded: flagged, kept in bounds
-                set_error(err, MPS_ERR_LIST_OVERFLOW);
-                off = 0;
-                val = 0.0;
-            }
-            crow[pos] = (unsigned short)((run << kRunOffBits) | off);
-            vrow[pos] = val;
+            crow[pos] = j;
+            vrow[pos] = -v;
             if (mcv32) mcv32[moff[i] + pos] = make_int2(j, __float_as_int((float)(-v)));
         }
         cnt += __popc(m);
@@ -229,8 +215,7 @@ __global__ void k_source_hs(int n, int cap, double re, double n0, double dt,
 }
 
 struct CG {
-    const unsigned short* __restrict__ mcode;  // (run, offset) column codes
-    const int* __restrict__ lbase;             // kLapRuns first slots per row
+    const int* __restrict__ mcol;
     const double* __restrict__ mval;
     const int* __restrict__ mlen;
     const int* __restrict__ moff;
@@ -241,37 +226,29 @@ struct CG {
     const int2* __restrict__ mrow;  // (offset, length) per row; length -1: not an unknown
 };
 
-// (A v)_i with one warp on row i of the CSR matrix: coalesced column-code and
-// value streams, two independent accumulators per lane, gathers of v from
-// L2, butterfly sum in a fixed order; every lane returns the row's value.
-// The row's run bases sit in shared memory (kLapRuns per warp); a column is
-// its run's base plus the code's 12-bit offset, so a column costs 2 bytes
-// instead of 4.  The code and value streams are read once per product and
-// loaded evict-first (ld.global.cs), which keeps the gathered vector in
-// L1/L2.  Launch with kRedThreads threads per block.
+// (A v)_i with one warp on row i of the CSR matrix: coalesced column/value
+// streams, two independent accumulators per lane, gathers of v from L2,
+// butterfly sum in a fixed order; every lane returns the row's value.  (This
+// plain form runs at 32 registers; restructured or deeper-unrolled variants
+// measured 15-70% slower on B200.)  The column/value streams are read once
+// per product and loaded evict-first (ld.global.cs), which keeps the
+// gathered vector in L1/L2: 0.61 against 0.755 ms per launch after 700 steps
+// of the 1.6 M-particle dam, equal on its first steps.
 template <typename V>
 __device__ __forceinline__ double spmv_row(const CG& A, const Grp<kRowG>& q,
                                            const V* __restrict__ v, int i, int off, int L)
 {
-    __shared__ int run_base[kRedThreads / 32][kLapRuns];
-    int* sb = run_base[threadIdx.x >> 5];
-    __syncwarp();  // the previous row's bases are no longer read
-    if (q.lane < kLapRuns) sb[q.lane] = A.lbase[(size_t)i * kLapRuns + q.lane];
-    __syncwarp();
-    const unsigned short* __restrict__ c = A.mcode + off;
+    const int* __restrict__ c = A.mcol + off;
     const double* __restrict__ a = A.mval + off;
     double acc0 = 0.0, acc1 = 0.0;
     int k = q.lane;
     for (; k + kRowG < L; k += 2 * kRowG) {
-        const unsigned c0 = __ldcs(c + k), c1 = __ldcs(c + k + kRowG);
-        const double a0 = __ldcs(a + k), a1 = __ldcs(a + k + kRowG);
-        acc0 += a0 * (double)v[sb[c0 >> kRunOffBits] + (int)(c0 & kRunOffMask)];
-        acc1 += a1 * (double)v[sb[c1 >> kRunOffBits] + (int)(c1 & kRunOffMask)];
+        int c0 = __ldcs(c + k), c1 = __ldcs(c + k + kRowG);
+        double a0 = __ldcs(a + k), a1 = __ldcs(a + k + kRowG);
+        acc0 += a0 * (double)v[c0];
+        acc1 += a1 * (double)v[c1];
     }
-    if (k < L) {
-        const unsigned c0 = __ldcs(c + k);
-        acc0 += __ldcs(a + k) * (double)v[sb[c0 >> kRunOffBits] + (int)(c0 & kRunOffMask)];
-    }
+    if (k < L) acc0 += __ldcs(a + k) * (double)v[__ldcs(c + k)];
     double acc = q.sum(acc0 + acc1);
     return A.diag[i] * (double)v[i] + acc;
 }
@@ -297,22 +274,22 @@ __device__ __forceinline__ float spmv_row_warp32(const CG& A, const int2* __rest
     for (; k + 3 * kRowG < L; k += 4 * kRowG) {
         const int2 e0 = __ldcs(e + k), e1 = __ldcs(e + k + kRowG), e2 = __ldcs(e + k + 2 * kRowG),
                    e3 = __ldcs(e + k + 3 * kRowG);
-        acc0 += __int_as_float(e0.y) * v[e0.x];
-        acc1 += __int_as_float(e1.y) * v[e1.x];
-        acc2 += __int_as_float(e2.y) * v[e2.x];
-        acc3 += __int_as_float(e3.y) * v[e3.x];
+        acc0 = __fmaf_rn(__int_as_float(e0.y), v[e0.x], acc0);
+        acc1 = __fmaf_rn(__int_as_float(e1.y), v[e1.x], acc1);
+        acc2 = __fmaf_rn(__int_as_float(e2.y), v[e2.x], acc2);
+        acc3 = __fmaf_rn(__int_as_float(e3.y), v[e3.x], acc3);
     }
     for (; k + kRowG < L; k += 2 * kRowG) {
         const int2 e0 = __ldcs(e + k), e1 = __ldcs(e + k + kRowG);
-        acc0 += __int_as_float(e0.y) * v[e0.x];
-        acc1 += __int_as_float(e1.y) * v[e1.x];
+        acc0 = __fmaf_rn(__int_as_float(e0.y), v[e0.x], acc0);
+        acc1 = __fmaf_rn(__int_as_float(e1.y), v[e1.x], acc1);
     }
     if (k < L) {
         const int2 e0 = __ldcs(e + k);
-        acc2 += __int_as_float(e0.y) * v[e0.x];
+        acc2 = __fmaf_rn(__int_as_float(e0.y), v[e0.x], acc2);
     }
     float acc = q.sumf((acc0 + acc1) + (acc2 + acc3));
-    return (float)A.diag[i] * v[i] + acc;
+    return __fmaf_rn((float)A.diag[i], v[i], acc);
 }
 
 // r = b - A x, z = M^-1 r, p = z; partials of b.b, r.z, r.r
@@ -377,7 +354,7 @@ __global__ void k_cg_start_scalars(int nparts, const double* __restrict__ part, 
 }
 
 // s = A p and partial p.s; one warp per row
-__global__ void __launch_bounds__(256, 8) k_cg_spmv(CG A, const double* __restrict__ p, double* __restrict__ s,
+__global__ void k_cg_spmv(CG A, const double* __restrict__ p, double* __restrict__ s,
                           double* __restrict__ part, const int* __restrict__ flag)
 {
     __shared__ double sh[33];
@@ -808,8 +785,7 @@ int vmps_ppe_apply(mps_ctx* c, const double* x, double* y)
 {
     int sms = 0;
     VMPS_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-    CG G{c->mcode, c->lbase, c->mval, c->mlen, c->moff, c->diag, c->bcon, c->cap_l, c->n, 0, 0, 0,
-         c->mrow};
+    CG G{c->mcol, c->mval, c->mlen, c->moff, c->diag, c->bcon, c->cap_l, c->n, 0, 0, 0, c->mrow};
     k_apply<<<sms * 8, kRedThreads, 0, c->stream>>>(G, x, y);
     vmps_count_launch(1);
     VMPS_CUDA(c, cudaGetLastError());
@@ -855,14 +831,14 @@ int vmps_ppe(mps_ctx* c)
     const int w_bcon = (f.ppe_at_predicted && c->p4s_bcon) ? 1 : 0;
     if (f.dim == 3)
         k_assemble<3><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
-                                                  nsrc, warm, c->pnew, c->pold, c->moff, c->lbase,
-                                                  c->mcode, c->mval, c->mcv32, c->mlen, c->diag,
-                                                  c->source, w_bcon, c->mrow, c->d_err);
+                                                  nsrc, warm, c->pnew, c->pold, c->moff, c->mcol,
+                                                  c->mval, c->mcv32, c->mlen, c->diag, c->source,
+                                                  w_bcon, c->mrow);
     else
         k_assemble<2><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
-                                                  nsrc, warm, c->pnew, c->pold, c->moff, c->lbase,
-                                                  c->mcode, c->mval, c->mcv32, c->mlen, c->diag,
-                                                  c->source, w_bcon, c->mrow, c->d_err);
+                                                  nsrc, warm, c->pnew, c->pold, c->moff, c->mcol,
+                                                  c->mval, c->mcv32, c->mlen, c->diag, c->source,
+                                                  w_bcon, c->mrow);
     vmps_count_launch(1);
     if (f.srcopt) {
         // slot of particle id k: inv_id[k] (the sort's inv buffer is free here)
@@ -891,7 +867,7 @@ int vmps_ppe(mps_ctx* c)
     }
     // zero initial guess (the assembly zeroed pnew): r = b exactly, so the
     // start kernels skip the product A x0
-    CG G{c->mcode, c->lbase, c->mval, c->mlen, c->moff, c->diag, c->bcon, c->cap_l, n,
+    CG G{c->mcol, c->mval, c->mlen, c->moff, c->diag, c->bcon, c->cap_l, n,
          f.solver == 1 ? 1 : 0, nblk, warm == 0 ? 1 : 0, c->mrow};
     double tol2 = f.cg_tol * f.cg_tol;
     const bool batched = c->nscenes > 1;

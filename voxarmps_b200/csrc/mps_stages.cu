@@ -59,7 +59,7 @@ __global__ void k_pnd(int n, Lists L, const double4* __restrict__ P4, WK wk, int
     int len = L.len[i];
     double sum = 0.0;
     for (int k = q.lane; k < len; k += G) {
-        int j = (int)((unsigned)row[k] & kSlotMask);
+        int j = row[k];
         if (i == j) continue;
         double dx, dy, dz;
         double d2 = d2of<DIM>(pi, P4[j], dx, dy, dz);
@@ -105,7 +105,7 @@ __global__ void k_vfraction(int n, Lists L, const int* __restrict__ ptype,
     const int* row = row_of(L, I);
     int len = L.len[I];
     for (int k = q.lane; k < len; k += G) {
-        int J = (int)((unsigned)row[k] & kSlotMask);
+        int J = row[k];
         int pj = ptype[J];
         if (I == J || pj <= 0) continue;
         double w = 1.0;
@@ -140,7 +140,7 @@ __device__ __forceinline__ void grad_sums(const Grp<G>& q, const Lists& L, int I
     double4 pi = P4[I];
     double ui = un[I], vi = vn[I], wi = DIM == 3 ? wn[I] : 0.0;
     for (int k = q.lane; k < len; k += G) {
-        int j = (int)((unsigned)row[k] & kSlotMask);
+        int j = row[k];
         if (I == j) continue;
         double dx, dy, dz;
         double d2 = d2of<DIM>(pi, P4[j], dx, dy, dz);
@@ -274,7 +274,7 @@ __global__ void k_sps2(int n, Lists L, Phys P, const int* __restrict__ ptype,
     double ni = neut[i];
     double4 pi = P4[i];
     for (int k = q.lane; k < len; k += G) {
-        int j = (int)((unsigned)row[k] & kSlotMask);
+        int j = row[k];
         if (i == j) continue;
         double dx, dy, dz;
         double d2 = d2of<DIM>(pi, P4[j], dx, dy, dz);
@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(256, 5) k_predict_p(int n, Lists Ls, PredArgs 
     const int* row = row_of(Ls, I);
     int len = Ls.len[I];
     for (int k = q.lane; k < len; k += G) {
-        int J = (int)((unsigned)row[k] & kSlotMask);
+        int J = row[k];
         if (I == J) continue;
         double dx, dy, dz;
         double d2 = d2of<DIM>(pi, P4[J], dx, dy, dz);
@@ -396,28 +396,27 @@ k_predict32(int n, Lists Ll, PredArgs A, WKf wl, const double* __restrict__ meu,
         if (!(d2 > 0.f)) return;
         const float W = w_fast32<DIM>(wl, d2);
         float NEU = neu_same;
-        if (pnd_word_ptype(fj.w) != pI) {
+        if ((int)fj.w != pI) {
             const double mJ = meu[J];
             NEU = (float)(2 * mI * mJ / (mI + mJ) / rhoI);
         }
         const float du = W * (vj.x - vi.x), dv = W * (vj.y - vi.y);
-        s4 += du * NEU;
-        s5 += dv * NEU;
+        s4 = __fmaf_rn(du, NEU, s4);
+        s5 = __fmaf_rn(dv, NEU, s5);
         if (TURB) {
             s7 += du;
             s8 += dv;
         }
         if (DIM == 3) {
             const float dw = W * (vj.z - vi.z);
-            s6 += dw * NEU;
+            s6 = __fmaf_rn(dw, NEU, s6);
             if (TURB) s9 += dw;
         }
     };
     // two entries per lane in flight (k, k + G); the sums see them in list order
     for (int k = q.lane; k < len; k += 2 * kPred32G) {
         const bool two = k + kPred32G < len;
-        const int J0 = (int)((unsigned)row[k] & kSlotMask),
-                  J1 = two ? (int)((unsigned)row[k + kPred32G] & kSlotMask) : I;
+        const int J0 = row[k], J1 = two ? row[k + kPred32G] : I;
         const float4 f0 = P4f[J0], f1 = P4f[J1], v0 = U4f[J0], v1 = U4f[J1];
         add(J0, f0, v0);
         add(J1, f1, v1);
@@ -486,7 +485,7 @@ k_predict(int n, Lists Ll, PredArgs A, const double* __restrict__ meu,
     const int* row = row_of(Ll, I);
     int len = Ll.len[I];
     for (int k = q.lane; k < len; k += kPredG) {
-        int J = (int)((unsigned)row[k] & kSlotMask);
+        int J = row[k];
         if (I == J) continue;
         double4 pj = P4[J];
         double dx, dy, dz;
@@ -566,7 +565,7 @@ __global__ void k_phat(int n, Lists L, const double* __restrict__ pnew, double* 
     const int* row = row_of(L, I);
     int len = L.len[I];
     for (int k = q.lane; k < len; k += G) {
-        double pj = pnew[(unsigned)row[k] & kSlotMask];
+        double pj = pnew[row[k]];
         if (pj < mn) mn = pj;
     }
     mn = q.min(mn);
@@ -601,7 +600,7 @@ __global__ void __launch_bounds__(256, 5) k_pressgrad(int n, Lists L, GradArgs A
     const int* row = row_of(L, I);
     int len = L.len[I];
     for (int k = q.lane; k < len; k += G) {
-        int J = (int)((unsigned)row[k] & kSlotMask);
+        int J = row[k];
         if (I == J) continue;
         double dx, dy, dz;
         double d2 = d2of<DIM>(pi, P4s[J], dx, dy, dz);
@@ -772,7 +771,7 @@ __global__ void __launch_bounds__(256, 3) k_collision(int n, Lists L, CollArgs A
     const int* row = row_of(L, i);
     const int len = L.len[i];
     for (int k = q.lane; k < len; k += G) {
-        const int j = (int)((unsigned)row[k] & kSlotMask);
+        const int j = row[k];
         if (i == j) continue;
         double ex, ey, ez;
         if (d2of<DIM>(pi, P4[j], ex, ey, ez) < A.coll2) {
@@ -795,7 +794,7 @@ __global__ void __launch_bounds__(256, 3) k_collision(int n, Lists L, CollArgs A
     double acc[6] = {0, 0, 0, 0, 0, 0};
     if (total > 1) {  // several: the pre-collision state plus the sum of the replays' changes
         for (int k = q.lane; k < len; k += G) {
-            const int j = (int)((unsigned)row[k] & kSlotMask);
+            const int j = row[k];
             if (i == j) continue;
             double ex, ey, ez;
             const double4 pj = P4[j];
@@ -941,18 +940,15 @@ inline int group_blocks(long n, int G) { return (int)((n * G + kBlock - 1) / kBl
 
 }  // namespace
 
-// FP32 copies relative to (x0, y0, z0).  With ptype: w holds the particle's
-// pnd_cell_word (its kind and PND-grid cell), else w = 0.
+// FP32 copies relative to (x0, y0, z0); w = ptype when given, else 0
 __global__ void k_pack_f(int n, const double* __restrict__ x, const double* __restrict__ y,
                          const double* __restrict__ z, double x0, double y0, double z0,
-                         const int* __restrict__ ptype, const int* __restrict__ cell_s, int ncx,
-                         int ncxy, float4* __restrict__ P4f)
+                         const int* __restrict__ ptype, float4* __restrict__ P4f)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n)
         P4f[i] = make_float4((float)(x[i] - x0), (float)(y[i] - y0), (float)(z[i] - z0),
-                             ptype ? __uint_as_float(pnd_cell_word(ptype[i], cell_s[i], ncx, ncxy))
-                                   : 0.f);
+                             ptype ? (float)ptype[i] : 0.f);
 }
 
 int vmps_pack(mps_ctx* c)
@@ -960,12 +956,11 @@ int vmps_pack(mps_ctx* c)
     const mps_config& f = c->cfg;
     k_pack_f<<<grid_blocks(c->n), kBlock, 0, c->stream>>>(c->n, c->x, c->y, c->z, f.xmin, f.ymin,
                                                           f.dim == 3 ? f.zmin : 0.0, c->ptype,
-                                                          c->cell_s, c->gs.ncx,
-                                                          c->gs.ncx * c->gs.ncy, c->P4f);
+                                                          c->P4f);
     vmps_count_launch(1);
     if (f.precision == 1) {
         k_pack_f<<<grid_blocks(c->n), kBlock, 0, c->stream>>>(c->n, c->u, c->v, c->w, 0.0, 0.0,
-                                                              0.0, nullptr, nullptr, 0, 0, c->U4f);
+                                                              0.0, nullptr, c->U4f);
         vmps_count_launch(1);
     }
     k_pack<<<grid_blocks(c->n), kBlock, 0, c->stream>>>(c->n, c->x, c->y, c->z, c->ptype, c->P4);
