@@ -182,7 +182,10 @@ __global__ void k_gnn_enc(int n, const float* __restrict__ feat, const bf16* __r
     *(bf162*)(h0 + o) = __floats2bfloat162_rn(fmaxf(a0, 0.f), fmaxf(a1, 0.f));
 }
 
-// m_i = (sum over the list of i of h_j) / len_i, list order, FP32 sums
+// m_i = (sum over the list of i of h_j) / len_i, list order, FP32 sums.  A
+// warp per node, two channels per lane: the row's entries are loaded once
+// (a lane per entry) and handed out by shuffles, and four neighbours' rows
+// are gathered before they are added, so four gathers are in flight.
 __global__ void k_gnn_agg(int n, int cap, const int* __restrict__ nbr, const int* __restrict__ len,
                           const bf16* __restrict__ hin, bf16* __restrict__ mout)
 {
@@ -192,11 +195,29 @@ __global__ void k_gnn_agg(int n, int cap, const int* __restrict__ nbr, const int
     const int L = len[i];
     const int* row = nbr + (size_t)i * cap;
     float s0 = 0.f, s1 = 0.f;
-    for (int k = 0; k < L; k++) {
-        const int j = row[k];
-        const float2 v = __bfloat1622float2(*(const bf162*)(hin + (size_t)j * H + 2 * q.lane));
-        s0 = s0 + v.x;
-        s1 = s1 + v.y;
+    for (int b = 0; b < L; b += 32) {
+        const int mine = b + q.lane < L ? row[b + q.lane] : 0;
+        const int cnt = min(32, L - b);
+        int k = 0;
+        for (; k + 4 <= cnt; k += 4) {
+            float2 v[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int j = __shfl_sync(0xffffffffu, mine, k + u);
+                v[u] = __bfloat1622float2(*(const bf162*)(hin + (size_t)j * H + 2 * q.lane));
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                s0 = s0 + v[u].x;
+                s1 = s1 + v[u].y;
+            }
+        }
+        for (; k < cnt; k++) {
+            const int j = __shfl_sync(0xffffffffu, mine, k);
+            const float2 v = __bfloat1622float2(*(const bf162*)(hin + (size_t)j * H + 2 * q.lane));
+            s0 = s0 + v.x;
+            s1 = s1 + v.y;
+        }
     }
     if (L > 0) {
         s0 = s0 / (float)L;
@@ -608,12 +629,35 @@ __global__ void k_gnn_agg_b(int n, int cap, const int* __restrict__ nbr, const i
     const int* row = nbr + (size_t)j * cap;
     const size_t o = (size_t)j * H + 2 * q.lane;
     float s0 = 0.f, s1 = 0.f;
-    for (int k = 0; k < L; k++) {
-        const int i = row[k];
-        const float li = (float)max(len[i], 1);
-        const float2 v = *(const float2*)(dm + (size_t)i * H + 2 * q.lane);
-        s0 = s0 + v.x / li;
-        s1 = s1 + v.y / li;
+    // the row handed out by shuffles, four neighbours' gathers in flight,
+    // added in list order
+    for (int b = 0; b < L; b += 32) {
+        const int mine = b + q.lane < L ? row[b + q.lane] : 0;
+        const float lmine = b + q.lane < L ? (float)max(len[mine], 1) : 1.f;
+        const int cnt = min(32, L - b);
+        int k = 0;
+        for (; k + 4 <= cnt; k += 4) {
+            float2 v[4];
+            float li[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int i = __shfl_sync(0xffffffffu, mine, k + u);
+                li[u] = __shfl_sync(0xffffffffu, lmine, k + u);
+                v[u] = *(const float2*)(dm + (size_t)i * H + 2 * q.lane);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                s0 = s0 + v[u].x / li[u];
+                s1 = s1 + v[u].y / li[u];
+            }
+        }
+        for (; k < cnt; k++) {
+            const int i = __shfl_sync(0xffffffffu, mine, k);
+            const float li = __shfl_sync(0xffffffffu, lmine, k);
+            const float2 v = *(const float2*)(dm + (size_t)i * H + 2 * q.lane);
+            s0 = s0 + v.x / li;
+            s1 = s1 + v.y / li;
+        }
     }
     const float2 g = *(const float2*)(dself + o);
     *(float2*)(dprev + o) = make_float2(g.x + s0, g.y + s1);
