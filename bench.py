@@ -339,7 +339,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     cfg, case, scenes = build_case(args.scale, args.config, args.precision, rank, ws)
     split = scenes is not None and ws > 1  # the batch's scenes are shared out
-    mixed = cfg["precision"] == 1
+    mixed = cfg["precision"] >= 1
     n = len(case["x"])
     fp = int((case["ptype"] > 0).sum())
     guess = args.guess or ("learned" if args.config in (3, 4) and not args.scale else "previous")
@@ -507,7 +507,9 @@ def run_ours(args):
             "graph": bool(args.graph), "ms_per_step_profiled_eager": prof_ms / args.steps,
             "tuning": dict(tuning, autotuned=bool(args.autotune)),
             "ppe_ms_per_step": statistics.mean(ppe_ms), "cg_iters_mean": statistics.mean(iters),
-            "precision": "mixed (FP32 inner CG, FP64 dots/refinement)" if mixed else "fp64",
+            "precision": ({1: "mixed (FP32 inner CG, FP64 dots/refinement; FP32 viscous sums)",
+                           2: "mixed (FP32 inner CG, FP64 dots/refinement; FP32 viscous sums, "
+                              "PNUMSTAR and pressure gradient)"}.get(cfg["precision"], "fp64")),
             "cg_outer_mean": outer / args.steps,
             "cg_relres_last": relres, "status_bits": status,
             "stage_ms": {k[3:]: statistics.mean(v) for k, v in stage.items()},
@@ -627,7 +629,8 @@ def mixed_vs_fp64(vm, cfg, case, scenes, dev, steps):
     run of the same case after the same number of steps (not timed)."""
     import numpy as np
     out = {}
-    for prec in (1, 0):
+    mixed = cfg["precision"]
+    for prec in (mixed, 0):
         c = dict(cfg)
         c["precision"] = prec
         s = vm.Solver(c, case, device=dev)
@@ -645,9 +648,9 @@ def mixed_vs_fp64(vm, cfg, case, scenes, dev, steps):
     def rel(a, b):
         return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
     res = {"steps": steps, "norm": "max|mixed - fp64| / max|fp64|",
-           "p_after_1_step": rel(out[1]["p_step1"], out[0]["p_step1"])}
+           "p_after_1_step": rel(out[mixed]["p_step1"], out[0]["p_step1"])}
     for f in ("p", "x", "y", "z", "u", "v", "w"):
-        res[f] = rel(out[1][f], out[0][f])
+        res[f] = rel(out[mixed][f], out[0][f])
     return res
 
 
@@ -672,8 +675,9 @@ def main():
                     help="CG starting point (default: learned for configs 3 and 4)")
     ap.add_argument("--gnn-train-steps", type=int, default=300,
                     help="solver steps of online training for the learned guess")
-    ap.add_argument("--precision", type=int, default=None, choices=[0, 1],
-                    help="PPE precision (default: mixed for configs 2 and 4, FP64 otherwise)")
+    ap.add_argument("--precision", type=int, default=None, choices=[0, 1, 2],
+                    help="0 FP64; 1 mixed PPE and FP32 viscous sums (default for configs 2 "
+                         "and 4); 2 as 1 with FP32 PNUMSTAR and pressure gradient")
     ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2, 3, 4],
                     help="benchmark configuration (1: the headline 3D dam break)")
     ap.add_argument("--advance", type=int, default=0,

@@ -75,7 +75,9 @@ typedef struct mps_config {
     int collision_gather; /* must be 1: order-independent collision */
     double xmin, xmax, ymin, ymax, zmin, zmax;  /* grown bounding box (main.cu:692-715) */
     /* B200 path knobs (no reference counterpart) */
-    int precision;        /* 0 FP64 throughout; 1 mixed (FP32 streams + FP64 refinement) */
+    int precision;        /* 0 FP64 throughout; 1 mixed PPE (FP32 inner CG, FP64 dots and
+                             refinement) and FP32 viscous sums; 2 as 1, with PNUMSTAR and
+                             the pressure gradient in FP32 as well */
     int list_cap_s;       /* neighbour-list capacity per particle, 0 = automatic */
     int list_cap_l;
 } mps_config;

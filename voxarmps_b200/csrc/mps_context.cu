@@ -134,7 +134,10 @@ int validate(const mps_config& f, std::string& why)
     }
     if (f.solver != 1 && f.solver != 2) { why = "solver must be 1 (Jacobi-PCG) or 2 (CG)"; return MPS_ERR_ARG; }
     if (f.warm_start < 0 || f.warm_start > 2) { why = "warm_start must be 0, 1 or 2"; return MPS_ERR_ARG; }
-    if (f.precision != 0 && f.precision != 1) { why = "precision must be 0 (FP64) or 1 (mixed)"; return MPS_ERR_ARG; }
+    if (f.precision < 0 || f.precision > 2) {
+        why = "precision must be 0 (FP64), 1 (mixed PPE) or 2 (mixed PPE, FP32 PND* and gradient)";
+        return MPS_ERR_ARG;
+    }
     return MPS_OK;
 }
 
@@ -231,7 +234,11 @@ int allocate(mps_ctx* c)
     TRY(dalloc(c, &c->P4c, P));
     TRY(dalloc(c, &c->U4, P));
     TRY(dalloc(c, &c->P4f, P));
-    if (c->cfg.precision == 1) TRY(dalloc(c, &c->U4f, P));
+    if (c->cfg.precision >= 1) TRY(dalloc(c, &c->U4f, P));
+    if (c->cfg.precision == 2) {
+        TRY(dalloc(c, &c->P4sf, P));
+        TRY(dalloc(c, &c->PH32, P));
+    }
     TRY(dalloc(c, &c->PH, P));
     TRY(dalloc(c, &c->cnt_l, (size_t)c->gl.tnc + 2));
     TRY(dalloc(c, &c->cst_l, (size_t)c->gl.tnc + 2));
@@ -245,7 +252,7 @@ int allocate(mps_ctx* c)
     TRY(dalloc(c, &c->mrow, P));
     TRY(dalloc(c, &c->mcol, (size_t)c->cap_l * P));
     TRY(dalloc(c, &c->mval, (size_t)c->cap_l * P));
-    if (c->cfg.precision == 1) {
+    if (c->cfg.precision >= 1) {
         TRY(dalloc(c, &c->mcv32, (size_t)c->cap_l * P));
         float** ffields[] = {&c->ir_d, &c->ir_r, &c->ir_z, &c->ir_p, &c->ir_s};
         for (auto f : ffields) TRY(dalloc(c, f, P));

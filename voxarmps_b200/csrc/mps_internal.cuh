@@ -187,6 +187,8 @@ struct mps_ctx {
     double4 *P4 = nullptr, *P4s = nullptr, *P4c = nullptr, *U4 = nullptr;
     float4* P4f = nullptr;   // positions relative to the box minimum, FP32, w = ptype
     float4* U4f = nullptr;   // velocities, FP32 (mixed precision's viscous sums)
+    float4* P4sf = nullptr;  // precision 2: predicted positions relative to the box, FP32
+    float2* PH32 = nullptr;  // precision 2: (pnew, phat) in FP32
     double screen_abs = 0;   // bound on |d2_fp32 - d2_exact| for the screening test
     double2* PH = nullptr;
     // sort / cells

@@ -879,7 +879,7 @@ int vmps_ppe(mps_ctx* c)
     const bool graph = cap == cudaStreamCaptureStatusActive;
     cudaGraphConditionalHandle cond = 0;
     if (graph) VMPS_CUDA(c, cudaGraphConditionalHandleCreate(&cond, cgraph, 1, cudaGraphCondAssignDefault));
-    const bool mixed = f.precision == 1;
+    const bool mixed = f.precision >= 1;
     IR I{c->mcv32, c->ir_d, c->ir_r, c->ir_z, c->ir_p, c->ir_s};
     if (mixed) {
         k_ir_start<<<nblk, kRedThreads, 0, st>>>(G, I, c->source, c->pnew, c->cg_r, c->cg_part);
@@ -1006,7 +1006,7 @@ int vmps_ppe_finish(mps_ctx* c)
     c->ppe_pending = false;
     const mps_config& f = c->cfg;
     c->cg_iters = c->cg_flag_host[1];
-    c->cg_outer = f.precision == 1 ? c->cg_flag_host[3] : 0;
+    c->cg_outer = f.precision >= 1 ? c->cg_flag_host[3] : 0;
     if (c->profile) {
         // launches after convergence exit at once: count the working ones
         const int working = c->cg_iters + c->cg_outer;

@@ -367,18 +367,26 @@ k_predict32(int n, Lists Ll, PredArgs A, WKf wl, const double* __restrict__ meu,
             const double* __restrict__ t1, const double* __restrict__ t2,
             const double* __restrict__ t3, double* __restrict__ xs, double* __restrict__ ys,
             double* __restrict__ zs, double* __restrict__ us, double* __restrict__ vs,
-            double* __restrict__ ws, double4* __restrict__ P4s)
+            double* __restrict__ ws, double4* __restrict__ P4s, float4* __restrict__ P4sf,
+            double3 box0)
 {
     Grp<kPred32G> q;
     int I = (int)q.gid;
     if (I >= n) return;
     double4 pi = P4[I], ui4 = U4[I];
     int pI = (int)pi.w;
+    // precision 2: the predicted positions in FP32 too, relative to the box
+    auto put_f = [&](const double4& o) {
+        if (P4sf)
+            P4sf[I] = make_float4((float)(o.x - box0.x), (float)(o.y - box0.y),
+                                  DIM == 3 ? (float)(o.z - box0.z) : 0.f, o.w);
+    };
     if (pI <= 0) {
         if (q.lane == 0) {
             xs[I] = pi.x; ys[I] = pi.y; us[I] = ui4.x; vs[I] = ui4.y;
             if (DIM == 3) { zs[I] = pi.z; ws[I] = ui4.z; }
             P4s[I] = pi;
+            put_f(pi);
         }
         return;
     }
@@ -444,6 +452,7 @@ k_predict32(int n, Lists Ll, PredArgs A, WKf wl, const double* __restrict__ meu,
         zs[I] = o.z;
     }
     P4s[I] = o;
+    put_f(o);
 }
 
 // PREDICTION, second part: viscous Laplacian over the Laplacian list, one
@@ -556,7 +565,7 @@ __global__ void k_pressure_wc(int n, const int* __restrict__ ptype, const double
 // PHATCALC (functions.cu:207-224); also packs (pnew, phat) for the gradient
 template <int G>
 __global__ void k_phat(int n, Lists L, const double* __restrict__ pnew, double* __restrict__ phat,
-                       double2* __restrict__ PH)
+                       double2* __restrict__ PH, float2* __restrict__ PH32)
 {
     Grp<G> q;
     int I = (int)q.gid;
@@ -572,6 +581,7 @@ __global__ void k_phat(int n, Lists L, const double* __restrict__ pnew, double* 
     if (q.lane == 0) {
         phat[I] = mn;
         PH[I] = make_double2(pnew[I], mn);
+        if (PH32) PH32[I] = make_float2((float)pnew[I], (float)mn);
     }
 }
 
@@ -615,6 +625,82 @@ __global__ void __launch_bounds__(256, 5) k_pressgrad(int n, Lists L, GradArgs A
     sum1 = q.sum(sum1);
     sum2 = q.sum(sum2);
     if (DIM == 3) sum3 = q.sum(sum3);
+    if (q.lane != 0) return;
+    double c = A.coef / rho[I], VMAX = A.vmax, coeff = 2.0;
+    double uN = us[I] - c * sum1;
+    double vN = vs[I] - c * sum2;
+    if (fabs(uN) > coeff * VMAX) uN = VMAX;
+    if (vN > coeff * VMAX) vN = coeff * VMAX;
+    if (vN < -coeff * VMAX) vN = -coeff * VMAX;
+    un[I] = uN;
+    vn[I] = vN;
+    if (DIM == 3) {
+        double wN = ws[I] - c * sum3;
+        if (fabs(wN) > coeff * VMAX) wN = VMAX;
+        wn[I] = wN;
+    }
+}
+
+// Precision 2: PNUMSTAR (functions.cu:157-201) with FP32 positions relative
+// to the box, FP32 weights and an FP32 sum; n* is stored in FP64 and the
+// source (n* - n0) / n0 is formed from it in FP64.
+template <int DIM, int G>
+__global__ void k_pnd32(int n, Lists L, const float4* __restrict__ P4f, WKf wk,
+                        double* __restrict__ out)
+{
+    Grp<G> q;
+    int i = (int)q.gid;
+    if (i >= n) return;
+    const float4 pi = P4f[i];
+    const int* row = row_of(L, i);
+    int len = L.len[i];
+    float sum = 0.f;
+    for (int k = q.lane; k < len; k += G) {
+        int j = row[k];
+        if (i == j) continue;
+        const float4 pj = P4f[j];
+        const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = DIM == 3 ? pj.z - pi.z : 0.f;
+        const float d2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+        if (d2 > 0.f) sum += w_fast32<DIM>(wk, d2);
+    }
+    sum = q.sumf(sum);
+    if (q.lane == 0) out[i] = (double)sum;
+}
+
+// Precision 2: PRESSGRAD (functions.cu:245-355) with FP32 positions,
+// pressures, weights and sums; u^{n+1} = u* - c * sum formed in FP64.
+template <int DIM, int G>
+__global__ void __launch_bounds__(256, 5) k_pressgrad32(int n, Lists L, GradArgs A, WKf wk,
+                            const int* __restrict__ ptype, const float2* __restrict__ PH32,
+                            const float4* __restrict__ P4sf, const double* __restrict__ rho,
+                            const double* __restrict__ us, const double* __restrict__ vs,
+                            const double* __restrict__ ws, double* __restrict__ un,
+                            double* __restrict__ vn, double* __restrict__ wn)
+{
+    Grp<G> q;
+    int I = (int)q.gid;
+    if (I >= n || ptype[I] <= 0) return;
+    float s1 = 0.f, s2 = 0.f, s3 = 0.f;
+    const float4 pi = P4sf[I];
+    const float2 phI = PH32[I];
+    const int* row = row_of(L, I);
+    int len = L.len[I];
+    for (int k = q.lane; k < len; k += G) {
+        int J = row[k];
+        if (I == J) continue;
+        const float4 pj = P4sf[J];
+        const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = DIM == 3 ? pj.z - pi.z : 0.f;
+        const float d2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+        if (!(d2 > 0.f)) continue;
+        const float2 phJ = PH32[J];
+        const float pp = (A.kh == 1) ? phJ.x + phI.x - (phI.y + phJ.y) : phJ.x - phI.y;
+        const float f = pp * w_fast32<DIM>(wk, d2) / d2;
+        s1 = __fmaf_rn(dx, f, s1);
+        s2 = __fmaf_rn(dy, f, s2);
+        if (DIM == 3) s3 = __fmaf_rn(dz, f, s3);
+    }
+    const double sum1 = q.sum((double)s1), sum2 = q.sum((double)s2);
+    const double sum3 = DIM == 3 ? q.sum((double)s3) : 0.0;
     if (q.lane != 0) return;
     double c = A.coef / rho[I], VMAX = A.vmax, coeff = 2.0;
     double uN = us[I] - c * sum1;
@@ -958,7 +1044,7 @@ int vmps_pack(mps_ctx* c)
                                                           f.dim == 3 ? f.zmin : 0.0, c->ptype,
                                                           c->P4f);
     vmps_count_launch(1);
-    if (f.precision == 1) {
+    if (f.precision >= 1) {
         k_pack_f<<<grid_blocks(c->n), kBlock, 0, c->stream>>>(c->n, c->u, c->v, c->w, 0.0, 0.0,
                                                               0.0, nullptr, c->U4f);
         vmps_count_launch(1);
@@ -983,6 +1069,9 @@ int vmps_pnd(mps_ctx* c, int at_star, int correct, int which, double* out)
             k_pnd<2, 32><<<group_blocks(c->n, 32), kBlock, 0, c->stream>>>(
                 c->n, lists(c, 0), P, wk, correct, c->cfg.ncorrection, out, c->d_max);
         vmps_count_launch(1);
+    } else if (at_star && !correct && c->cfg.precision == 2 && c->P4sf) {
+        // precision 2: n* from the FP32 predicted positions
+        LAUNCH_SMALL(k_pnd32, c->n, lists(c, 1), c->P4sf, make_wkf(wk), out);
     } else {
         LAUNCH_SMALL(k_pnd, c->n, lists(c, 1), P, wk, correct, c->cfg.ncorrection, out, c->d_max);
     }
@@ -1051,14 +1140,14 @@ int vmps_predict(mps_ctx* c)
     k_predict32<D, T><<<group_blocks(c->n, kPred32G), kBlock, 0, c->stream>>>(                 \
         c->n, lists(c, 0), A, make_wkf(A.wl), c->meu, c->P4, c->U4, c->P4f, c->U4f, c->pres_x, \
         c->pres_y, c->pres_z, c->neut, c->t1, c->t2, c->t3, c->xs, c->ys, c->zs, c->us, c->vs,  \
-        c->ws, c->P4s)
+        c->ws, c->P4s, c->P4sf, make_double3(f.xmin, f.ymin, f.dim == 3 ? f.zmin : 0.0))
 #define PRED64(D, T)                                                                          \
     k_predict<D, T><<<group_blocks(c->n, kPredG), kBlock, 0, c->stream>>>(                     \
         c->n, lists(c, 0), A, c->meu, c->P4, c->U4, c->pres_x, c->pres_y, c->pres_z, c->neut,  \
         c->t1, c->t2, c->t3, c->xs, c->ys, c->zs, c->us, c->vs, c->ws, c->P4s)
     const bool turb = f.turb != 0;
     c->p4s_bcon = false;  // P4s.w is ptype again until BCON
-    if (f.precision == 1) {  // FP32 neighbour sums
+    if (f.precision >= 1) {  // FP32 neighbour sums
         if (f.dim == 3) { if (turb) PRED32(3, true); else PRED32(3, false); }
         else { if (turb) PRED32(2, true); else PRED32(2, false); }
     } else {
@@ -1088,13 +1177,13 @@ int vmps_phat(mps_ctx* c)
     const int G = (c->cfg.dim == 3 ? SmallG<3>::G : SmallG<2>::G) * (c->tune_small_wide ? 2 : 1);
     if (G == 16)
         k_phat<16><<<group_blocks(c->n, 16), kBlock, 0, c->stream>>>(c->n, lists(c, 1), c->pnew,
-                                                                     c->phat, c->PH);
+                                                                     c->phat, c->PH, c->PH32);
     else if (G == 8)
         k_phat<8><<<group_blocks(c->n, 8), kBlock, 0, c->stream>>>(c->n, lists(c, 1), c->pnew,
-                                                                   c->phat, c->PH);
+                                                                   c->phat, c->PH, c->PH32);
     else
         k_phat<4><<<group_blocks(c->n, 4), kBlock, 0, c->stream>>>(c->n, lists(c, 1), c->pnew,
-                                                                   c->phat, c->PH);
+                                                                   c->phat, c->PH, c->PH32);
     vmps_count_launch(1);
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
@@ -1108,8 +1197,12 @@ int vmps_pressgrad(mps_ctx* c)
     A.coef = f.relaxp * (2.0 * f.dt / c->n0_s);
     A.vmax = f.vmax;
     A.kh = f.kh;
-    LAUNCH_SMALL(k_pressgrad, c->n, lists(c, 1), A, c->ptype, c->PH, c->P4s, c->rho, c->us, c->vs,
-               c->ws, c->un, c->vn, c->wn);
+    if (f.precision == 2)
+        LAUNCH_SMALL(k_pressgrad32, c->n, lists(c, 1), A, make_wkf(A.wk), c->ptype, c->PH32,
+                     c->P4sf, c->rho, c->us, c->vs, c->ws, c->un, c->vn, c->wn);
+    else
+        LAUNCH_SMALL(k_pressgrad, c->n, lists(c, 1), A, c->ptype, c->PH, c->P4s, c->rho, c->us,
+                     c->vs, c->ws, c->un, c->vn, c->wn);
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
 }
