@@ -152,10 +152,40 @@ int mps_get_state(mps_ctx* ctx, double* x, double* y, double* z, double* u, doub
                   double* w, double* p);
 /* Overwrite one state array between stage calls, host doubles in the caller's
  * particle order: x y z u v w (the packed copies the stages read follow),
- * p, pnew, un vn wn (the corrected velocity COLLISION2 and PREPDATA read).
+ * p, pnew, un vn wn (the corrected velocity COLLISION2 and PREPDATA read),
+ * phat (the previous step's, read by PREDICTION), pold (p^(n-1)).
  * The reference's caller owns these arrays and may write them between any
  * two calls of main.cu's loop (main.cu:1027-1363); this is that write. */
 int mps_set_field(mps_ctx* ctx, const char* field, const double* in);
+/* ---- one scene split between contexts (slab decomposition) -------------- *
+ * No counterpart in the reference (one process, one scene).  Each context
+ * holds the particles of one slab of the scene plus ghost copies of its
+ * neighbours' particles near the slab faces (voxarmps_b200/slab.py drives
+ * it).  mps_set_owned: 1 for the particles this context owns, 0 for ghosts
+ * (caller order; all 1 after mps_upload); ghost rows stay out of this
+ * context's PPE system but remain columns of the owned rows.  mps_set_n0
+ * replaces n0 (the scene's, formed over all contexts).  mps_get_rows /
+ * mps_set_rows read / write one double field (names as mps_download, plus
+ * "cg_p", the CG direction) at the given caller-order indices: the ghost
+ * exchanges.  The PPE then runs host-driven, FP64 Jacobi-PCG only
+ * (precision 0, method 1): mps_ppe_assemble (MATRIX, source, initial
+ * guess), mps_dcg_start (local b.b, r.z, r.r), and per iteration
+ * mps_dcg_spmv (local p.s), mps_dcg_update (local r.z, r.r after x += a p,
+ * r -= a s), mps_dcg_direction (p = z + b p); the caller sums the local
+ * values over the contexts and exchanges the ghost entries of pnew and
+ * cg_p between the calls; mps_dcg_finish clamps and records the outcome
+ * (bb: the scene's b.b). */
+int mps_set_owned(mps_ctx* ctx, const int* owned);
+int mps_set_n0(mps_ctx* ctx, double n0_s, double n0_l);
+int mps_get_rows(mps_ctx* ctx, const char* field, int count, const int* ids, double* out);
+int mps_set_rows(mps_ctx* ctx, const char* field, int count, const int* ids, const double* in);
+int mps_ppe_assemble(mps_ctx* ctx);
+int mps_dcg_start(mps_ctx* ctx, double* local3);
+int mps_dcg_spmv(mps_ctx* ctx, double* local_ps);
+int mps_dcg_update(mps_ctx* ctx, double alpha, double* local2);
+int mps_dcg_direction(mps_ctx* ctx, double beta);
+int mps_dcg_finish(mps_ctx* ctx, int iters, double relres, double bb);
+
 /* Per-stage device timing with CUDA events (off by default).  While on,
  * scalars ms_neighbors ms_explicit ms_ppe ms_post ms_step (last step) and
  * spmv_ms / spmv_launches, lists_ms (accumulated) are available. */

@@ -49,6 +49,8 @@ EXPORTS = [
     "mps_gnn_create", "mps_gnn_use", "mps_gnn_train", "mps_gnn_params", "mps_gnn_features",
     "mps_gnn_forward", "mps_gnn_download", "mps_get_tuning", "mps_set_tuning", "mps_autotune",
     "mps_snapshot_vtu", "mps_wait_io", "mps_save_checkpoint", "mps_load_checkpoint",
+    "mps_set_owned", "mps_set_n0", "mps_get_rows", "mps_set_rows", "mps_ppe_assemble",
+    "mps_dcg_start", "mps_dcg_spmv", "mps_dcg_update", "mps_dcg_direction", "mps_dcg_finish",
 ]
 
 _LIB = None
@@ -119,6 +121,16 @@ def load_library(path: str = LIB_PATH):
                                    C.POINTER(C.c_double)]
     lib.mps_cell_order_noalloc.argtypes = [C.POINTER(MpsConfig), C.c_double, C.c_int, P, P, P,
                                            P, P, P, P]
+    lib.mps_set_owned.argtypes = [P, IP]
+    lib.mps_set_n0.argtypes = [P, C.c_double, C.c_double]
+    lib.mps_get_rows.argtypes = [P, C.c_char_p, C.c_int, IP, DP]
+    lib.mps_set_rows.argtypes = [P, C.c_char_p, C.c_int, IP, DP]
+    lib.mps_ppe_assemble.argtypes = [P]
+    lib.mps_dcg_start.argtypes = [P, DP]
+    lib.mps_dcg_spmv.argtypes = [P, DP]
+    lib.mps_dcg_update.argtypes = [P, C.c_double, DP]
+    lib.mps_dcg_direction.argtypes = [P, C.c_double]
+    lib.mps_dcg_finish.argtypes = [P, C.c_int, C.c_double, C.c_double]
     _LIB = lib
     return lib
 
@@ -266,6 +278,56 @@ class Solver:
         if a.shape != (self.n,):
             raise ValueError(f"{name}: expected {self.n} values")
         return self._chk(self.lib.mps_set_field(self.h, name.encode(), _dp(a)), f"set {name}")
+
+    # ---- one scene split between contexts (voxarmps_b200/slab.py) -------
+    def set_owned(self, owned):
+        o = np.ascontiguousarray(owned, np.int32)
+        return self._chk(self.lib.mps_set_owned(self.h, o.ctypes.data_as(C.POINTER(C.c_int))),
+                         "set_owned")
+
+    def set_n0(self, n0_s: float, n0_l: float):
+        return self._chk(self.lib.mps_set_n0(self.h, n0_s, n0_l), "set_n0")
+
+    def get_rows(self, name: str, ids) -> np.ndarray:
+        i = np.ascontiguousarray(ids, np.int32)
+        out = np.empty(len(i), np.float64)
+        self._chk(self.lib.mps_get_rows(self.h, name.encode(), len(i),
+                                        i.ctypes.data_as(C.POINTER(C.c_int)), _dp(out)),
+                  f"get_rows {name}")
+        return out
+
+    def set_rows(self, name: str, ids, values):
+        i = np.ascontiguousarray(ids, np.int32)
+        v = np.ascontiguousarray(values, np.float64)
+        if len(v) != len(i):
+            raise ValueError("one value per index")
+        return self._chk(self.lib.mps_set_rows(self.h, name.encode(), len(i),
+                                               i.ctypes.data_as(C.POINTER(C.c_int)), _dp(v)),
+                         f"set_rows {name}")
+
+    def ppe_assemble(self):
+        return self._chk(self.lib.mps_ppe_assemble(self.h), "ppe_assemble")
+
+    def dcg_start(self) -> np.ndarray:
+        out = np.zeros(3)
+        self._chk(self.lib.mps_dcg_start(self.h, _dp(out)), "dcg_start")
+        return out
+
+    def dcg_spmv(self) -> float:
+        out = np.zeros(1)
+        self._chk(self.lib.mps_dcg_spmv(self.h, _dp(out)), "dcg_spmv")
+        return float(out[0])
+
+    def dcg_update(self, alpha: float) -> np.ndarray:
+        out = np.zeros(2)
+        self._chk(self.lib.mps_dcg_update(self.h, alpha, _dp(out)), "dcg_update")
+        return out
+
+    def dcg_direction(self, beta: float):
+        return self._chk(self.lib.mps_dcg_direction(self.h, beta), "dcg_direction")
+
+    def dcg_finish(self, iters: int, relres: float, bb: float):
+        return self._chk(self.lib.mps_dcg_finish(self.h, iters, relres, bb), "dcg_finish")
 
     def get_state(self, *ptrs):
         return self._chk(self.lib.mps_get_state(self.h, *[p or None for p in ptrs]), "get_state")

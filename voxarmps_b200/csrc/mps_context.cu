@@ -172,10 +172,46 @@ __global__ void k_permute_in(int n, const int* __restrict__ oid, const double* _
     if (b) b[i] = v;
 }
 
+__global__ void k_permute_in_i(int n, const int* __restrict__ oid, const int* __restrict__ in,
+                               int* __restrict__ a)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = in[oid[i]];
+}
+
+__global__ void k_slot_of(int n, const int* __restrict__ oid, int* __restrict__ slot_of)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) slot_of[oid[i]] = i;
+}
+
+// rows by particle index; an index outside [0, n) is reported, not followed
+__global__ void k_rows(int count, int n, const int* __restrict__ ids,
+                       const int* __restrict__ slot_of, double* __restrict__ a,
+                       double* __restrict__ vals, int set, unsigned int* err)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const int id = ids[k];
+    if (id < 0 || id >= n) {
+        atomicOr(err, (unsigned)MPS_ERR_ARG);
+        return;
+    }
+    const int s = slot_of[id];
+    if (set) a[s] = vals[k];
+    else vals[k] = a[s];
+}
+
 __global__ void k_iota(int n, int* a)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) a[i] = i;
+}
+
+__global__ void k_fill_i(int n, int v, int* a)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
 }
 
 __global__ void k_density(int n, const int* __restrict__ ptype, double rho1, double rho2,
@@ -222,7 +258,9 @@ int allocate(mps_ctx* c)
                           &c->cg_p, &c->cg_s, &c->xc, &c->yc, &c->zc, &c->uc, &c->vc, &c->wc,
                           &c->pres_x, &c->pres_y, &c->pres_z};
     for (auto f : dfields) TRY(dalloc(c, f, P));
-    int** ifields[] = {&c->ptype, &c->oid, &c->scene, &c->bcon, &c->cell_l, &c->cell_s, &c->bpos_l,
+    int** ifields[] = {&c->ptype, &c->oid, &c->scene, &c->own, &c->sysmask, &c->stage_ids,
+                       &c->slot_of,
+                       &c->bcon, &c->cell_l, &c->cell_s, &c->bpos_l,
                        &c->bpos_s, &c->bslot_l, &c->boid_l, &c->bslot_s, &c->boid_s, &c->src,
                        &c->inv, &c->perm_s, &c->perm_s_tmp, &c->len_l, &c->len_s, &c->mlen,
                        &c->moff};
@@ -262,23 +300,23 @@ int allocate(mps_ctx* c)
     // CG partials: 5 arrays of one value per block, at most 8 blocks per SM
     c->cg_part_cap = (size_t)5 * 8 * sms;
     TRY(dalloc(c, &c->cg_part, c->cg_part_cap));
-    TRY(dalloc(c, &c->cg_scal, 16));
+    TRY(dalloc(c, &c->cg_scal, 32));
     TRY(dalloc(c, &c->cg_flag, 4));
     TRY(dalloc(c, &c->d_err, 1));
     TRY(dalloc(c, &c->len_max, 2));
     TRY(dalloc(c, &c->d_max, 1));
     TRY(halloc(c, &c->cg_flag_host, 4));
-    TRY(halloc(c, &c->red_host, 16));
+    TRY(halloc(c, &c->red_host, 32));
     TRY(halloc(c, &c->h_err, 1));
     // alternates of the persistent fields for the reorder (same order as
-    // persistent_set in mps_neighbors.cu: 15 doubles then 5 ints)
+    // persistent_set in mps_neighbors.cu: 15 doubles then 6 ints)
     c->alts.clear();
     for (int k = 0; k < 15; k++) {
         double* q;
         TRY(dalloc(c, &q, P));
         c->alts.push_back(q);
     }
-    for (int k = 0; k < 5; k++) {
+    for (int k = 0; k < 6; k++) {
         int* q;
         TRY(dalloc(c, &q, P));
         c->alts.push_back(q);
@@ -294,7 +332,8 @@ double* field_d(mps_ctx* c, const std::string& f)
         {"wn", c->wn}, {"xs", c->xs}, {"ys", c->ys}, {"zs", c->zs}, {"us", c->us},
         {"vs", c->vs}, {"ws", c->ws}, {"n", c->nd}, {"nstar", c->nds}, {"C", c->C},
         {"meu", c->meu}, {"neut", c->neut}, {"t1", c->t1}, {"t2", c->t2}, {"t3", c->t3},
-        {"rho", c->rho}, {"source", c->source}, {"diag", c->diag}, {"pold", c->pold}};
+        {"rho", c->rho}, {"source", c->source}, {"diag", c->diag}, {"pold", c->pold},
+        {"cg_p", c->cg_p}};
     for (auto& e : t)
         if (f == e.n) return e.p;
     return nullptr;
@@ -429,8 +468,9 @@ int mps_upload(mps_ctx* c, int n, const double* x, const double* y, const double
     VMPS_CUDA(c, up(c->p, p));
     VMPS_CUDA(c, cudaMemcpyAsync(c->ptype, ptype, sizeof(int) * n, cudaMemcpyHostToDevice, st));
     k_iota<<<grid_blocks(n), kBlock, 0, st>>>(n, c->oid);
+    k_fill_i<<<grid_blocks(n), kBlock, 0, st>>>(n, 1, c->own);
     k_density<<<grid_blocks(n), kBlock, 0, st>>>(n, c->ptype, f.rho1, f.rho2, c->rho);
-    vmps_count_launch(2);
+    vmps_count_launch(3);
     VMPS_CUDA(c, cudaStreamSynchronize(st));
     c->initialized = false;
     c->steps = 0;
@@ -819,8 +859,8 @@ int mps_set_field(mps_ctx* c, const char* field, const double* in)
 {
     NEED_INIT(c);
     if (!field || !in) return MPS_ERR_ARG;
-    static const char* const kSettable[] = {"x", "y", "z",    "u",  "v",  "w",
-                                            "p", "pnew", "un", "vn", "wn"};
+    static const char* const kSettable[] = {"x", "y", "z",  "u",  "v",  "w",    "p",
+                                            "pnew", "un", "vn", "wn", "phat", "pold"};
     std::string f(field);
     bool ok = false;
     for (const char* s : kSettable) ok = ok || f == s;
@@ -839,6 +879,79 @@ int mps_set_field(mps_ctx* c, const char* field, const double* in)
     if (f == "x" || f == "y" || f == "z" || f == "u" || f == "v" || f == "w") TRY(vmps_pack(c));
     VMPS_CUDA(c, cudaStreamSynchronize(c->stream));
     return MPS_OK;
+}
+
+// ---- slab decomposition support --------------------------------------------
+
+int mps_set_owned(mps_ctx* c, const int* owned)
+{
+    NEED_INIT(c);
+    if (!owned) return MPS_ERR_ARG;
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    const int n = c->n;
+    VMPS_CUDA(c, cudaMemcpyAsync(c->stage_ids, owned, sizeof(int) * n, cudaMemcpyHostToDevice,
+                                 c->stream));
+    k_permute_in_i<<<grid_blocks(n), kBlock, 0, c->stream>>>(n, c->oid, c->stage_ids, c->own);
+    vmps_count_launch(1);
+    drop_graphs(c);
+    VMPS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MPS_OK;
+}
+
+int mps_set_n0(mps_ctx* c, double n0_s, double n0_l)
+{
+    NEED_INIT(c);
+    if (!(n0_s > 0) || !(n0_l > 0)) return MPS_ERR_ARG;
+    c->n0_s = n0_s;
+    c->n0_l = n0_l;
+    drop_graphs(c);
+    return MPS_OK;
+}
+
+// rows by caller-order index: out[k] = field[particle ids[k]] (get) or
+// field[particle ids[k]] = in[k] (set)
+static int rows_io(mps_ctx* c, const char* field, int count, const int* ids, double* out,
+                   const double* in)
+{
+    NEED_INIT(c);
+    double* a = field ? field_d(c, field) : nullptr;
+    if (!a || count < 0 || count > c->n || (count > 0 && !ids) || (count > 0 && !out && !in)) {
+        c->msg = std::string("rows: bad field or arguments");
+        return MPS_ERR_ARG;
+    }
+    if (count == 0) return MPS_OK;
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    const int n = c->n;
+    k_slot_of<<<grid_blocks(n), kBlock, 0, st>>>(n, c->oid, c->slot_of);
+    VMPS_CUDA(c, cudaMemcpyAsync(c->stage_ids, ids, sizeof(int) * count, cudaMemcpyHostToDevice,
+                                 st));
+    if (in)
+        VMPS_CUDA(c, cudaMemcpyAsync(c->stage_in, in, sizeof(double) * count,
+                                     cudaMemcpyHostToDevice, st));
+    k_rows<<<grid_blocks(count), kBlock, 0, st>>>(count, n, c->stage_ids, c->slot_of, a,
+                                                  c->stage_in, in ? 1 : 0, c->d_err);
+    vmps_count_launch(2);
+    if (out)
+        VMPS_CUDA(c, cudaMemcpyAsync(out, c->stage_in, sizeof(double) * count,
+                                     cudaMemcpyDeviceToHost, st));
+    VMPS_CUDA(c, cudaStreamSynchronize(st));
+    if (in && (!strcmp(field, "x") || !strcmp(field, "y") || !strcmp(field, "z") ||
+               !strcmp(field, "u") || !strcmp(field, "v") || !strcmp(field, "w")))
+        TRY(vmps_pack(c));
+    return MPS_OK;
+}
+
+int mps_get_rows(mps_ctx* c, const char* field, int count, const int* ids, double* out)
+{
+    if (!out && count > 0) return MPS_ERR_ARG;
+    return rows_io(c, field, count, ids, out, nullptr);
+}
+
+int mps_set_rows(mps_ctx* c, const char* field, int count, const int* ids, const double* in)
+{
+    if (!in && count > 0) return MPS_ERR_ARG;
+    return rows_io(c, field, count, ids, nullptr, in);
 }
 
 int mps_get_state(mps_ctx* c, double* x, double* y, double* z, double* u, double* v, double* w,

@@ -148,6 +148,7 @@ struct mps_ctx {
     int cg_iters = 0;
     int cg_loop_kernels = 4, cg_nspmv = 0;
     bool ppe_pending = false;
+    int ppe_warm = 1;  // initial guess of the last assembly (0: zero)
     // CUDA graph of one step per buffer parity (the reorder double-buffers
     // the persistent state, so the step's pointers alternate with period 2)
     bool use_graph = false;
@@ -165,6 +166,14 @@ struct mps_ctx {
     double *p = nullptr, *pnew = nullptr, *phat = nullptr, *un = nullptr, *vn = nullptr,
            *wn = nullptr, *rho = nullptr, *nd = nullptr, *pold = nullptr;
     int *ptype = nullptr, *oid = nullptr, *scene = nullptr;
+    // slab decomposition: 1 for the particles this context owns, 0 for ghost
+    // copies of a neighbouring rank's particles (all 1 in a single context)
+    int* own = nullptr;
+    // rows outside this context's PPE system: bcon != 0 or a ghost (the CG
+    // kernels' row mask; equal to bcon when every particle is owned)
+    int* sysmask = nullptr;
+    int* stage_ids = nullptr;  // H2D staging of particle indices (row exchanges)
+    int* slot_of = nullptr;    // slot of each caller-order particle index
     // batched scenes (nscenes == 1: one scene, the global box)
     int nscenes = 1;
     double* sbox = nullptr;     // 6 per scene

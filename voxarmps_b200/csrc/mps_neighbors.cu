@@ -500,7 +500,7 @@ static void persistent_set(mps_ctx* ctx, GatherSet& g, std::vector<void**>& slot
     slots.clear();
     double** d[] = {&ctx->x, &ctx->y, &ctx->z, &ctx->u, &ctx->v, &ctx->w, &ctx->p, &ctx->pnew,
                     &ctx->phat, &ctx->un, &ctx->vn, &ctx->wn, &ctx->rho, &ctx->nd, &ctx->pold};
-    int** ii[] = {&ctx->ptype, &ctx->oid, &ctx->cell_l, &ctx->cell_s, &ctx->scene};
+    int** ii[] = {&ctx->ptype, &ctx->oid, &ctx->cell_l, &ctx->cell_s, &ctx->scene, &ctx->own};
     for (auto f : d) {
         g.from[g.count] = *f;
         g.elem[g.count] = 8;

@@ -83,12 +83,15 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
                            int* __restrict__ mcol, double* __restrict__ mval,
                            int2* __restrict__ mcv32, int* __restrict__ mlen,
                            double* __restrict__ diag, double* __restrict__ source, int w_bcon,
-                           int2* __restrict__ mrow)
+                           int2* __restrict__ mrow, const int* __restrict__ own,
+                           int* __restrict__ sysmask)
 {
     Grp<kAsmG> q;
     int i = (int)q.gid;
     if (i >= n) return;
     int bi = bcon[i];
+    const bool mine = own[i] != 0;
+    if (q.lane == 0) sysmask[i] = (bi != 0 || !mine) ? 1 : 0;
     if (bi != 0) {
         if (q.lane == 0) {
             mlen[i] = 0;
@@ -97,6 +100,15 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
             source[i] = 0.0;
             if (warm == 2) pold[i] = pnew[i];
             pnew[i] = 0.0;
+        }
+        return;
+    }
+    if (!mine) {  // a ghost: its row belongs to its owner's system, its value arrives
+        if (q.lane == 0) {  // from the owner (a column here, not a row)
+            mlen[i] = 0;
+            mrow[i] = make_int2(moff[i], -1);
+            diag[i] = 0.0;
+            source[i] = 0.0;
         }
         return;
     }
@@ -785,14 +797,18 @@ int vmps_ppe_apply(mps_ctx* c, const double* x, double* y)
 {
     int sms = 0;
     VMPS_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-    CG G{c->mcol, c->mval, c->mlen, c->moff, c->diag, c->bcon, c->cap_l, c->n, 0, 0, 0, c->mrow};
+    CG G{c->mcol, c->mval, c->mlen, c->moff, c->diag, c->sysmask, c->cap_l, c->n, 0, 0, 0, c->mrow};
     k_apply<<<sms * 8, kRedThreads, 0, c->stream>>>(G, x, y);
     vmps_count_launch(1);
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
 }
 
-int vmps_ppe(mps_ctx* c)
+// PRESSURECALC's assembly part (MATRIX, source, initial guess); the solve
+// follows in vmps_ppe or, for a scene split between contexts, in the
+// host-driven CG entry points below.  *warm_out: the initial guess used
+// (0: zero, the start kernels then skip the product).
+static int ppe_assemble(mps_ctx* c, int* warm_out)
 {
     const mps_config& f = c->cfg;
     cudaStream_t st = c->stream;
@@ -833,12 +849,12 @@ int vmps_ppe(mps_ctx* c)
         k_assemble<3><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
                                                   nsrc, warm, c->pnew, c->pold, c->moff, c->mcol,
                                                   c->mval, c->mcv32, c->mlen, c->diag, c->source,
-                                                  w_bcon, c->mrow);
+                                                  w_bcon, c->mrow, c->own, c->sysmask);
     else
         k_assemble<2><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
                                                   nsrc, warm, c->pnew, c->pold, c->moff, c->mcol,
                                                   c->mval, c->mcv32, c->mlen, c->diag, c->source,
-                                                  w_bcon, c->mrow);
+                                                  w_bcon, c->mrow, c->own, c->sysmask);
     vmps_count_launch(1);
     if (f.srcopt) {
         // slot of particle id k: inv_id[k] (the sort's inv buffer is free here)
@@ -854,20 +870,43 @@ int vmps_ppe(mps_ctx* c)
                                              c->vs, c->ws, c->source);
         vmps_count_launch(1);
     }
+    *warm_out = warm;
+    return MPS_OK;
+}
+
+// grid of the CG kernels: blocks per SM from the autotuner, else as many as
+// fit (at most 8); cg_part holds [0,3*nblk) start/update partials and
+// [4*nblk,5*nblk) p.s
+static int cg_grid(mps_ctx* c, int* out)
+{
     int nblk = 0, occ = 0;
     VMPS_CUDA(c, cudaDeviceGetAttribute(&nblk, cudaDevAttrMultiProcessorCount, c->device));
     VMPS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg_spmv, kRedThreads, 0));
-    // blocks per SM: the autotuner's choice, else as many as fit (at most 8)
     const int bps = c->tune_cg_bps > 0 ? c->tune_cg_bps : 8;
     nblk *= std::max(1, std::min(occ, bps));
-    // layout of cg_part: [0,3*nblk) start/update partials, [4*nblk,5*nblk) p.s
     if ((size_t)5 * nblk > c->cg_part_cap) {
         c->msg = "CG partial buffer too small for the launch grid";
         return MPS_ERR_ARG;
     }
+    *out = nblk;
+    return MPS_OK;
+}
+
+int vmps_ppe(mps_ctx* c)
+{
+    const mps_config& f = c->cfg;
+    cudaStream_t st = c->stream;
+    const int n = c->n;
+    int warm = 0, nblk = 0;
+    {
+        int r = ppe_assemble(c, &warm);
+        if (r != MPS_OK) return r;
+        r = cg_grid(c, &nblk);
+        if (r != MPS_OK) return r;
+    }
     // zero initial guess (the assembly zeroed pnew): r = b exactly, so the
     // start kernels skip the product A x0
-    CG G{c->mcol, c->mval, c->mlen, c->moff, c->diag, c->bcon, c->cap_l, n,
+    CG G{c->mcol, c->mval, c->mlen, c->moff, c->diag, c->sysmask, c->cap_l, n,
          f.solver == 1 ? 1 : 0, nblk, warm == 0 ? 1 : 0, c->mrow};
     double tol2 = f.cg_tol * f.cg_tol;
     const bool batched = c->nscenes > 1;
@@ -893,7 +932,7 @@ int vmps_ppe(mps_ctx* c)
     }
     vmps_count_launch(2);
     if (batched) {
-        k_scene_sums<<<c->nscenes, kRedThreads, 0, st>>>(0, c->sfirst, c->slast, c->scene, c->bcon,
+        k_scene_sums<<<c->nscenes, kRedThreads, 0, st>>>(0, c->sfirst, c->slast, c->scene, c->sysmask,
                                                          c->source, tol2, c->sbb, nullptr, nullptr,
                                                          nullptr);
         vmps_count_launch(1);
@@ -914,7 +953,7 @@ int vmps_ppe(mps_ctx* c)
             if (c->profile && !graph) VMPS_CUDA(c, cudaEventRecord(c->ev_spmv[2 * k + 1], s));
             if (batched)
                 k_scene_sums<<<c->nscenes, kRedThreads, 0, s>>>(2, c->sfirst, c->slast, c->scene,
-                                                                c->bcon, c->cg_r, tol2, c->sbb,
+                                                                c->sysmask, c->cg_r, tol2, c->sbb,
                                                                 c->srr, c->sok, c->cg_flag);
             k_ir_update<<<nblk, kRedThreads, 0, s>>>(G, I, c->cg_r, c->cg_part + 4 * nblk,
                                                      c->cg_part, c->cg_scal, c->cg_flag);
@@ -933,7 +972,7 @@ int vmps_ppe(mps_ctx* c)
                                                  c->cg_flag);
         if (batched)
             k_scene_sums<<<c->nscenes, kRedThreads, 0, s>>>(1, c->sfirst, c->slast, c->scene,
-                                                            c->bcon, c->cg_r, tol2, c->sbb,
+                                                            c->sysmask, c->cg_r, tol2, c->sbb,
                                                             c->srr, c->sok, c->cg_flag);
         k_cg_direction<<<nblk, kRedThreads, 0, s>>>(G, c->cg_z, c->cg_p, c->cg_part, c->cg_scal,
                                                     c->cg_flag, tol2, f.cg_max, c->nscenes,
@@ -1025,3 +1064,184 @@ int vmps_ppe_finish(mps_ctx* c)
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Host-driven Jacobi-PCG over this context's rows, for a scene split between
+// contexts (slab decomposition, voxarmps_b200/slab.py).  Each entry point
+// runs one part of an iteration on the rows this context owns and returns
+// the rank-local sums it formed (fixed-order block partials, then a fixed
+// order over the blocks); the caller adds them over the ranks, forms alpha
+// and beta, and between the calls exchanges the ghost entries of the CG
+// vectors (mps_get_rows / mps_set_rows on "pnew" and "cg_p").  With one
+// context the sequence reproduces vmps_ppe's FP64 Jacobi-PCG.
+namespace {
+
+__global__ void k_local_sums(int nparts, int count, const double* __restrict__ part,
+                             double* __restrict__ out)
+{
+    __shared__ double sh[33];
+    for (int k = 0; k < count; k++) {
+        const double v = reduce_parts(part + (size_t)k * nparts, nparts, sh);
+        if (threadIdx.x == 0) out[k] = v;
+    }
+}
+
+// x += alpha p; r -= alpha s; z = M^-1 r; partials r.z, r.r (rows of this context)
+__global__ void __launch_bounds__(256, 8) k_dcg_update(CG A, double alpha, double* __restrict__ x,
+                                                       double* __restrict__ r,
+                                                       double* __restrict__ zv,
+                                                       const double* __restrict__ p,
+                                                       const double* __restrict__ s,
+                                                       double* __restrict__ part)
+{
+    __shared__ double sh[33];
+    double rz = 0, rr = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+        if (A.bcon[i] != 0) continue;
+        const double xi = x[i] + alpha * p[i];
+        const double ri = r[i] - alpha * s[i];
+        const double zi = A.precond ? ri / A.diag[i] : ri;
+        x[i] = xi;
+        r[i] = ri;
+        zv[i] = zi;
+        rz += ri * zi;
+        rr += ri * ri;
+    }
+    rz = block_sum(rz, sh);
+    rr = block_sum(rr, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = rz;
+        part[A.nparts + blockIdx.x] = rr;
+    }
+}
+
+// p = z + beta p on the rows of this context
+__global__ void k_dcg_direction(CG A, double beta, const double* __restrict__ zv,
+                                double* __restrict__ p)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x)
+        if (A.bcon[i] == 0) p[i] = zv[i] + beta * p[i];
+}
+
+__global__ void k_set_zero_flag(double* scal, double bb)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) scal[S_ZERO] = (bb == 0.0) ? 1.0 : 0.0;
+}
+
+CG dcg_args(mps_ctx* c, int nblk)
+{
+    return CG{c->mcol, c->mval, c->mlen, c->moff, c->diag, c->sysmask, c->cap_l, c->n,
+              c->cfg.solver == 1 ? 1 : 0, nblk, c->ppe_warm == 0 ? 1 : 0, c->mrow};
+}
+
+// the first `count` partial arrays of part, summed, to the host
+int local_sums_to_host(mps_ctx* c, int nblk, const double* part, int count, double* out)
+{
+    // cg_scal / red_host slots 16..19 (the device loop's scalars use 0..15)
+    k_local_sums<<<1, kRedThreads, 0, c->stream>>>(nblk, count, part, c->cg_scal + 16);
+    vmps_count_launch(1);
+    VMPS_CUDA(c, cudaMemcpyAsync(c->red_host + 16, c->cg_scal + 16, sizeof(double) * count,
+                                 cudaMemcpyDeviceToHost, c->stream));
+    VMPS_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < count; k++) out[k] = c->red_host[16 + k];
+    return MPS_OK;
+}
+
+}  // namespace
+
+#define DCG_NEED(c)                                                                 \
+    do {                                                                            \
+        if (!(c) || !(c)->initialized || (c)->cfg.method == 3 || (c)->cfg.precision != 0) \
+            return MPS_ERR_ARG;                                                     \
+    } while (0)
+
+extern "C" {
+
+int mps_ppe_assemble(mps_ctx* c)
+{
+    DCG_NEED(c);
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    int warm = 0;
+    int r = ppe_assemble(c, &warm);
+    if (r != MPS_OK) return r;
+    c->ppe_warm = warm;
+    VMPS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MPS_OK;
+}
+
+int mps_dcg_start(mps_ctx* c, double* local3)
+{
+    DCG_NEED(c);
+    if (!local3) return MPS_ERR_ARG;
+    int nblk = 0;
+    int r = cg_grid(c, &nblk);
+    if (r != MPS_OK) return r;
+    const CG G = dcg_args(c, nblk);
+    VMPS_CUDA(c, cudaMemsetAsync(c->cg_flag, 0, 4 * sizeof(int), c->stream));
+    k_cg_start<<<nblk, kRedThreads, 0, c->stream>>>(G, c->source, c->pnew, c->cg_r, c->cg_z,
+                                                     c->cg_p, c->cg_part);
+    vmps_count_launch(1);
+    return local_sums_to_host(c, nblk, c->cg_part, 3, local3);  // b.b, r.z, r.r
+}
+
+int mps_dcg_spmv(mps_ctx* c, double* local_ps)
+{
+    DCG_NEED(c);
+    if (!local_ps) return MPS_ERR_ARG;
+    int nblk = 0;
+    int r = cg_grid(c, &nblk);
+    if (r != MPS_OK) return r;
+    const CG G = dcg_args(c, nblk);
+    k_cg_spmv<<<nblk, kRedThreads, 0, c->stream>>>(G, c->cg_p, c->cg_s, c->cg_part + 4 * nblk,
+                                                    c->cg_flag);
+    vmps_count_launch(1);
+    return local_sums_to_host(c, nblk, c->cg_part + 4 * nblk, 1, local_ps);
+}
+
+int mps_dcg_update(mps_ctx* c, double alpha, double* local2)
+{
+    DCG_NEED(c);
+    if (!local2) return MPS_ERR_ARG;
+    int nblk = 0;
+    int r = cg_grid(c, &nblk);
+    if (r != MPS_OK) return r;
+    const CG G = dcg_args(c, nblk);
+    k_dcg_update<<<nblk, kRedThreads, 0, c->stream>>>(G, alpha, c->pnew, c->cg_r, c->cg_z,
+                                                       c->cg_p, c->cg_s, c->cg_part);
+    vmps_count_launch(1);
+    return local_sums_to_host(c, nblk, c->cg_part, 2, local2);  // r.z, r.r
+}
+
+int mps_dcg_direction(mps_ctx* c, double beta)
+{
+    DCG_NEED(c);
+    int nblk = 0;
+    int r = cg_grid(c, &nblk);
+    if (r != MPS_OK) return r;
+    k_dcg_direction<<<nblk, kRedThreads, 0, c->stream>>>(dcg_args(c, nblk), beta, c->cg_z, c->cg_p);
+    vmps_count_launch(1);
+    VMPS_CUDA(c, cudaGetLastError());
+    return MPS_OK;
+}
+
+int mps_dcg_finish(mps_ctx* c, int iters, double relres, double bb)
+{
+    DCG_NEED(c);
+    const mps_config& f = c->cfg;
+    k_set_zero_flag<<<1, 32, 0, c->stream>>>(c->cg_scal, bb);
+    k_clamp<<<grid_blocks(c->n), kBlock, 0, c->stream>>>(c->n, f.pmin, f.pmax, c->cg_scal, c->pnew,
+                                                          nullptr, c->spmax, c->sbb);
+    vmps_count_launch(2);
+    VMPS_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->cg_iters = iters;
+    c->cg_outer = 0;
+    c->cg_relres = relres;
+    c->ppe_pending = false;
+    if (!(relres <= f.cg_tol)) {
+        c->host_err |= MPS_ERR_NOT_CONVERGED;
+        return MPS_ERR_NOT_CONVERGED;
+    }
+    return MPS_OK;
+}
+
+}  // extern "C"
