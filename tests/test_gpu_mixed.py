@@ -104,12 +104,15 @@ def test_mixed_batched_scenes_each_converged():
     g.close()
 
 
-# precision 2 against the FP64 run after 10 steps of the 3D dam at the
-# benchmark spacing (max-norm relative): FP32 positions relative to the box
-# carry about 1e-7 m absolute error, which n* turns into a source error of a
-# few 1e-5 relative to n0 -- percent-level in (n* - n0)/n0 -- and the
-# pressure follows it
-FP32_EXPLICIT_P = 5e-1
+# precision 2 against the FP64 run after 10 steps (max-norm relative):
+# measured p 1.4e-4 / 3.9e-5, u 7e-5 / 4e-5, x 1e-7 / 2e-7 on the 2D dam /
+# the 12,608-particle 3D dam.  FP32 positions relative to the box carry
+# about 1e-7 m of rounding, which n* turns into noise of a few 1e-6 of n0
+# in the source (n* - n0)/n0; on the 1.6 M-particle dam, where the box is
+# larger and the fluid starts at rest, that noise is as large as the first
+# step's pressure (bench.py --config 2 --precision 2 reports it)
+FP32_EXPLICIT_P = 1e-3
+FP32_EXPLICIT_U = 1e-3
 FP32_EXPLICIT_X = 1e-6
 
 
@@ -134,5 +137,7 @@ def test_fp32_pnd_and_gradient_against_fp64(which):
     print(f"\nprecision 2 vs FP64 after 10 steps ({which}): " +
           ", ".join(f"{k} {v:.2e}" for k, v in errs.items()))
     assert errs["p"] <= FP32_EXPLICIT_P
+    for f in ("u", "v", "w"):
+        assert errs[f] <= FP32_EXPLICIT_U, f
     for f in ("x", "y", "z"):
         assert errs[f] <= FP32_EXPLICIT_X, f

@@ -421,6 +421,309 @@ __global__ void __launch_bounds__(kTcThreads) k_gnn_layer_tc(
                      "r"(kTcCols));
 }
 
+// ---- the backward products on the tensor cores (TF32) -------------------
+// The gradients are FP32, so both backward products run tcgen05.mma of
+// kind::tf32 (FP32 operands rounded to TF32's 10-bit mantissa, FP32
+// accumulation): du = W^T dz per node tile (k_gnn_layer_b_tc) and the
+// weight gradient sum over nodes of dz u^T per block of nodes
+// (k_gnn_wgrad_tc).  Operands use the same no-swizzle K-major layout as the
+// forward with 4-byte elements: a core matrix is 8 rows x 4 values.
+__device__ __forceinline__ uint32_t core_offset32(int r, int k, int R)
+{
+    return (uint32_t)(((((k >> 2) * (R >> 3)) + (r >> 3)) << 7) + ((r & 7) << 4) + ((k & 3) << 2));
+}
+
+// kind::tf32 instruction descriptor: D FP32, A and B TF32 (format 2), K-major
+__host__ __device__ constexpr uint32_t tf32_idesc(int M, int N)
+{
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t idesc,
+                                         uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* v)
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+          "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t slot_addr, uint32_t cols)
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot_addr),
+                 "r"(cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t tmem, uint32_t cols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(cols));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+        bar));
+}
+
+constexpr uint32_t kTbCols = 2 * H;  // du: 128 FP32 columns
+struct TbSmem {
+    float a[kTcM * H];       // dz of the node tile (M = 128 nodes, K = 64)
+    float b[2 * H * H];      // W^T (N = 128 inputs, K = 64 outputs)
+    unsigned long long bar;
+    uint32_t tmem;
+};
+constexpr size_t kTbSmemBytes = sizeof(TbSmem) + 128;
+
+// Backward through h_out = h_in + relu(z), z = W [h_in, m] + b, for 128
+// nodes at a time: dz = dh_out * [z > 0] (also written out for the weight
+// gradient), du = W^T dz on the tensor cores, dself = dh_out + du[0, H),
+// dm = du[H, 2H).
+__global__ void __launch_bounds__(kTcThreads) k_gnn_layer_b_tc(
+    int n, const bf16* __restrict__ w16, int offW, const bf16* __restrict__ z,
+    const float* __restrict__ dhout, float* __restrict__ dz, float* __restrict__ dself,
+    float* __restrict__ dm, unsigned int* err)
+{
+    extern __shared__ unsigned char tc_raw[];
+    TbSmem& S = *reinterpret_cast<TbSmem*>((reinterpret_cast<uintptr_t>(tc_raw) + 127) &
+                                           ~(uintptr_t)127);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t a_addr = smem_addr(S.a), b_addr = smem_addr(S.b), bar = smem_addr(&S.bar);
+    // B: row k (input), column c (output) = W[c][k]
+    for (int e = tid; e < 2 * H * H; e += kTcThreads) {
+        const int c = e / (2 * H), k = e % (2 * H);
+        *reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(S.b) + core_offset32(k, c, 2 * H)) =
+            __bfloat162float(w16[offW + e]);
+    }
+    if (warp == 0) tmem_alloc(smem_addr(&S.tmem), kTbCols);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = S.tmem;
+    const int tiles = (n + kTcM - 1) / kTcM;
+    uint32_t parity = 0;
+    bool failed = false;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const int node0 = t * kTcM;
+        // dz of the tile, four outputs at a time; rows past n are zero
+        for (int e = tid; e < kTcM * (H / 4); e += kTcThreads) {
+            const int c4 = e / kTcM, r = e % kTcM, node = node0 + r;
+            float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (node < n) {
+                const size_t o = (size_t)node * H + 4 * c4;
+                const float4 g = *reinterpret_cast<const float4*>(dhout + o);
+                const float2 z01 = __bfloat1622float2(*reinterpret_cast<const bf162*>(z + o));
+                const float2 z23 = __bfloat1622float2(*reinterpret_cast<const bf162*>(z + o + 2));
+                d = make_float4(z01.x > 0.f ? g.x : 0.f, z01.y > 0.f ? g.y : 0.f,
+                                z23.x > 0.f ? g.z : 0.f, z23.y > 0.f ? g.w : 0.f);
+                *reinterpret_cast<float4*>(dz + o) = d;
+            }
+            *reinterpret_cast<float4*>(reinterpret_cast<unsigned char*>(S.a) +
+                                       core_offset32(r, 4 * c4, kTcM)) = d;
+        }
+        asm volatile("fence.proxy.async.shared::cta;");
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (tid == 0) {
+#pragma unroll
+            for (int s = 0; s < H / 8; s++)
+                mma_tf32(tmem, umma_desc(a_addr + s * 2 * (kTcM * 16), kTcM * 16, 128),
+                         umma_desc(b_addr + s * 2 * (2 * H * 16), 2 * H * 16, 128),
+                         tf32_idesc(kTcM, 2 * H), s > 0 ? 1u : 0u);
+            umma_commit(bar);
+        }
+        failed = !mbar_wait(bar, parity);
+        parity ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (__syncthreads_or(failed)) {
+            failed = true;
+            break;
+        }
+        const int r = warp * 32 + lane, node = node0 + r;
+#pragma unroll
+        for (int kb = 0; kb < 2 * H; kb += 16) {
+            uint32_t v[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)kb, v);
+            if (node < n) {
+#pragma unroll
+                for (int j = 0; j < 16; j += 4) {
+                    const int k = kb + j;
+                    const float4 du = make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]),
+                                                  __uint_as_float(v[j + 2]),
+                                                  __uint_as_float(v[j + 3]));
+                    if (k < H) {
+                        const size_t o = (size_t)node * H + k;
+                        const float4 g = *reinterpret_cast<const float4*>(dhout + o);
+                        *reinterpret_cast<float4*>(dself + o) =
+                            make_float4(g.x + du.x, g.y + du.y, g.z + du.z, g.w + du.w);
+                    } else {
+                        *reinterpret_cast<float4*>(dm + (size_t)node * H + (k - H)) = du;
+                    }
+                }
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;");
+    }
+    if (failed) {
+        if (tid == 0) atomicOr(err, (unsigned)MPS_ERR_CUDA);
+        mbar_wait(bar, parity ^ 1u);
+    }
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, kTbCols);
+}
+
+// Weight gradient of a layer (C = H outputs, K = 2H inputs [h, m]) over the
+// block's fixed range of nodes, 32 nodes per MMA chunk: D[k][c] = sum over
+// nodes of u[k] dz[c] in a 128 x 64 FP32 accumulator (M = the inputs, N =
+// the outputs, K = the nodes; both operands transposed into K-major tiles as
+// they are staged).  gb[c] = sum over nodes of dz[c] in FP32, fixed order.
+// Writes the block's partial in the parameters' layout (W row-major, then
+// b) for k_gnn_reduce.
+constexpr int kWgChunk = 32;  // nodes per MMA chunk (four K = 8 steps)
+struct WgSmem {
+    float a[2 * H * kWgChunk];  // u^T: M = 128 inputs, K = 32 nodes
+    float b[H * kWgChunk];      // dz^T: N = 64 outputs, K = 32 nodes
+    float bsum[kTcThreads][4];  // per-thread bias partials
+    unsigned long long bar;
+    uint32_t tmem;
+};
+constexpr size_t kWgSmemBytes = sizeof(WgSmem) + 128;
+
+__global__ void __launch_bounds__(kTcThreads) k_gnn_wgrad_tc(
+    int n, const float* __restrict__ dz, const bf16* __restrict__ u0, const bf16* __restrict__ u1,
+    float* __restrict__ part, unsigned int* err)
+{
+    extern __shared__ unsigned char tc_raw[];
+    WgSmem& S = *reinterpret_cast<WgSmem*>((reinterpret_cast<uintptr_t>(tc_raw) + 127) &
+                                           ~(uintptr_t)127);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int C = H, K = 2 * H, E = C * K + C;
+    const uint32_t a_addr = smem_addr(S.a), b_addr = smem_addr(S.b), bar = smem_addr(&S.bar);
+    const int per = ((n + gridDim.x - 1) / gridDim.x + kWgChunk - 1) / kWgChunk * kWgChunk;
+    const int i0 = min(n, blockIdx.x * per), i1 = min(n, i0 + per);
+    if (warp == 0) tmem_alloc(smem_addr(&S.tmem), (uint32_t)H);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = S.tmem;
+    // bias partials: thread t sums outputs 4 (t % 16) .. +3 over the nodes
+    // t / 16, t / 16 + 8, ... of every chunk, in chunk order
+    float bs[4] = {0.f, 0.f, 0.f, 0.f};
+    uint32_t parity = 0;
+    bool failed = false, any = false;
+    for (int c0 = i0; c0 < i1; c0 += kWgChunk) {
+        // u^T: 8 inputs of one node per item (BF16 -> FP32)
+        for (int e = tid; e < kWgChunk * (K / 8); e += kTcThreads) {
+            const int a = e % kWgChunk, k8 = e / kWgChunk, node = c0 + a;
+            float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            if (node < i1) {
+                const bf16* src = k8 < H / 8 ? u0 + (size_t)node * H + 8 * k8
+                                             : u1 + (size_t)node * H + 8 * (k8 - H / 8);
+                const uint4 raw = *reinterpret_cast<const uint4*>(src);
+                const bf162* h2 = reinterpret_cast<const bf162*>(&raw);
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const float2 f = __bfloat1622float2(h2[q]);
+                    v[2 * q] = f.x;
+                    v[2 * q + 1] = f.y;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                *reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(S.a) +
+                                          core_offset32(8 * k8 + q, a, K)) = v[q];
+        }
+        // dz^T: 4 outputs of one node per item
+        for (int e = tid; e < kWgChunk * (C / 4); e += kTcThreads) {
+            const int c4 = e % (C / 4), a = e / (C / 4), node = c0 + a;
+            float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (node < i1) d = *reinterpret_cast<const float4*>(dz + (size_t)node * C + 4 * c4);
+            const float dv[4] = {d.x, d.y, d.z, d.w};
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                *reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(S.b) +
+                                          core_offset32(4 * c4 + q, a, C)) = dv[q];
+                bs[q] += dv[q];
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;");
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (tid == 0) {
+#pragma unroll
+            for (int s = 0; s < kWgChunk / 8; s++)
+                mma_tf32(tmem, umma_desc(a_addr + s * 2 * (K * 16), K * 16, 128),
+                         umma_desc(b_addr + s * 2 * (C * 16), C * 16, 128), tf32_idesc(K, C),
+                         (any || s > 0) ? 1u : 0u);
+            umma_commit(bar);
+        }
+        any = true;
+        failed = !mbar_wait(bar, parity);
+        parity ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (__syncthreads_or(failed)) {
+            failed = true;
+            break;
+        }
+        // the chunk's tiles are free again for the next chunk
+    }
+    // bias: the 8 threads of each output group in thread order
+#pragma unroll
+    for (int q = 0; q < 4; q++) S.bsum[tid][q] = bs[q];
+    __syncthreads();
+    float* out = part + (size_t)blockIdx.x * E;
+    if (tid < C / 4) {
+        float g[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int t = tid; t < kTcThreads; t += C / 4)
+            for (int q = 0; q < 4; q++) g[q] += S.bsum[t][q];
+        for (int q = 0; q < 4; q++) out[C * K + 4 * tid + q] = g[q];
+    }
+    // W: input k = TMEM lane k, output c = column c
+    if (!failed) {
+        const int k = warp * 32 + lane;
+#pragma unroll
+        for (int cb = 0; cb < C; cb += 16) {
+            uint32_t v[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, v);
+#pragma unroll
+            for (int j = 0; j < 16; j++) out[(size_t)(cb + j) * K + k] = any ? __uint_as_float(v[j]) : 0.f;
+        }
+    } else {
+        if (tid == 0) atomicOr(err, (unsigned)MPS_ERR_CUDA);
+        mbar_wait(bar, parity ^ 1u);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, (uint32_t)H);
+}
+
 // y = bd + wd . h_L, sequential over channels; thread per node
 __global__ void k_gnn_dec(int n, const bf16* __restrict__ w16, Layout Y, const bf16* __restrict__ hL,
                           float* __restrict__ y)
@@ -565,55 +868,6 @@ __global__ void k_gnn_dy_resid(int n, const double* __restrict__ ar, const int* 
     dy[i] = unknown_fluid(bcon[i], ptype[i])
                 ? (float)(-2.0 * (double)scal[0] * ar[i] * (double)scal[3])
                 : 0.f;
-}
-
-// Backward through h_out = h_in + relu(z), z = W [h_in, m] + b:
-// dz = dh_out * [z > 0]; du = W^T dz (sequential over outputs c);
-// dself = dh_out + du[0, H); dm = du[H, 2H).  Warp per node.
-__global__ void __launch_bounds__(kThreads) k_gnn_layer_b(int n, const bf16* __restrict__ w16, int offW,
-                                                          const bf16* __restrict__ z,
-                                                          const float* __restrict__ dhout,
-                                                          float* __restrict__ dz,
-                                                          float* __restrict__ dself,
-                                                          float* __restrict__ dm)
-{
-    __shared__ float W[H][2 * H];
-    __shared__ float zs[kThreads / 32][H];
-    for (int e = threadIdx.x; e < 2 * H * H; e += blockDim.x)
-        W[e / (2 * H)][e % (2 * H)] = __bfloat162float(w16[offW + e]);
-    __syncthreads();
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int nw = gridDim.x * (blockDim.x >> 5);
-    float* d = zs[wib];
-    for (int i = blockIdx.x * (blockDim.x >> 5) + wib; i < n; i += nw) {
-        const size_t o = (size_t)i * H + 2 * lane;
-        const float2 zv = __bfloat1622float2(*(const bf162*)(z + o));
-        const float2 g = *(const float2*)(dhout + o);
-        const float d0 = zv.x > 0.f ? g.x : 0.f, d1 = zv.y > 0.f ? g.y : 0.f;
-        *(float2*)(dz + o) = make_float2(d0, d1);
-        d[2 * lane] = d0;
-        d[2 * lane + 1] = d1;
-        __syncwarp();
-        // lane owns inputs k = 4 lane .. 4 lane + 3
-        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-        for (int c = 0; c < H; c++) {
-            const float dc = d[c];
-            const float4 w = *(const float4*)&W[c][4 * lane];
-            a0 = a0 + w.x * dc;
-            a1 = a1 + w.y * dc;
-            a2 = a2 + w.z * dc;
-            a3 = a3 + w.w * dc;
-        }
-        __syncwarp();
-        const int k = 4 * lane;
-        if (k < H) {
-            const float4 gself = *(const float4*)(dhout + (size_t)i * H + k);
-            *(float4*)(dself + (size_t)i * H + k) =
-                make_float4(gself.x + a0, gself.y + a1, gself.z + a2, gself.w + a3);
-        } else {
-            *(float4*)(dm + (size_t)i * H + (k - H)) = make_float4(a0, a1, a2, a3);
-        }
-    }
 }
 
 // transpose of the mean aggregation on a symmetric list:
@@ -841,6 +1095,11 @@ int tc_prepare(mps_ctx* c)
     if (c->device >= 0 && c->device < 64 && done[c->device]) return MPS_OK;
     VMPS_CUDA(c, cudaFuncSetAttribute(k_gnn_layer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kTcSmemBytes));
+    VMPS_CUDA(c, cudaFuncSetAttribute(k_gnn_layer_b_tc,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kTbSmemBytes));
+    VMPS_CUDA(c, cudaFuncSetAttribute(k_gnn_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kWgSmemBytes));
     if (c->device >= 0 && c->device < 64) done[c->device] = true;
     return MPS_OK;
 }
@@ -919,14 +1178,17 @@ int backward(mps_ctx* c, vmps_gnn* G, int objective)
     GTRY(wgrad(c, G, 1, H, G->dz, 1, G->h + Y.L * NH, nullptr, nullptr, Y.wd));
     int sms = 0;
     VMPS_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-    const int lblocks = std::max(1, std::min(warp_blocks(n), sms * 4));
+    const int tc_blocks = std::max(1, std::min((n + kTcM - 1) / kTcM, sms * 3));
     float* d_out = G->dh;   // gradient w.r.t. h_l
     float* d_self = G->dh2;
     for (int l = Y.L - 1; l >= 0; l--) {
-        k_gnn_layer_b<<<lblocks, kThreads, 0, st>>>(n, G->w16, Y.W[l], G->z + (l + 1) * NH, d_out,
-                                                    G->dz, d_self, G->dm);
-        vmps_count_launch(1);
-        GTRY(wgrad(c, G, H, 2 * H, G->dz, H, G->h + l * NH, G->mm + l * NH, nullptr, Y.W[l]));
+        k_gnn_layer_b_tc<<<tc_blocks, kTcThreads, kTbSmemBytes, st>>>(
+            n, G->w16, Y.W[l], G->z + (l + 1) * NH, d_out, G->dz, d_self, G->dm, c->d_err);
+        k_gnn_wgrad_tc<<<kWgradBlocks, kTcThreads, kWgSmemBytes, st>>>(
+            n, G->dz, G->h + l * NH, G->mm + l * NH, G->part, c->d_err);
+        k_gnn_reduce<<<(2 * H * H + H + kThreads - 1) / kThreads, kThreads, 0, st>>>(
+            kWgradBlocks, 2 * H * H + H, G->part, G->g + Y.W[l]);
+        vmps_count_launch(3);
         // d_out <- dself + transpose-aggregated dm (gradient w.r.t. h_(l-1))
         k_gnn_agg_b<<<warp_blocks(n), kThreads, 0, st>>>(n, c->cap_s, c->nbr_s, c->len_s, d_self,
                                                          G->dm, d_out);
