@@ -343,9 +343,15 @@ def run_ours(args):
     n = len(case["x"])
     fp = int((case["ptype"] > 0).sum())
     guess = args.guess or ("learned" if args.config in (3, 4) and not args.scale else "previous")
-    trained = None
+    trained = own = None
     if guess == "learned":
-        trained = train_guess(vm, cfg, case, scenes, dev, args.gnn_train_steps)
+        source = args.guess_train or ("configs" if args.config == 3 and not args.scale else "own")
+        if source == "configs":
+            trained = train_guess_configs(vm, dev)
+            # the same network trained on the scene's own snapshots, for comparison
+            own = train_guess(vm, cfg, case, scenes, dev, args.gnn_train_steps)
+        else:
+            trained = train_guess(vm, cfg, case, scenes, dev, args.gnn_train_steps)
     if guess == "zero":
         cfg["warm_start"] = 0
     if guess == "extrapolated":
@@ -543,8 +549,11 @@ def run_ours(args):
         if trained is not None:
             line["guess_training"] = trained["info"]
             line["advanced_steps_before_warmup"] = args.gnn_train_steps
-            line["guess_comparison"] = compare_guesses(vm, cfg, case, scenes, dev,
-                                                       trained["params"], args)
+            if own is not None:
+                line["guess_training_own_scene"] = own["info"]
+            line["guess_comparison"] = compare_guesses(
+                vm, cfg, case, scenes, dev, trained["params"], args,
+                own=None if own is None else own["params"])
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -585,23 +594,73 @@ def train_guess(vm, cfg, case, scenes, dev, steps, iters=2, lr=2e-3):
                                 "and activations, FP32 sums"}}
 
 
-def compare_guesses(vm, cfg, case, scenes, dev, params, args, steps=20):
+def train_guess_configs(vm, dev, rounds=100, per_round=(20, 1, 1), iters=2, lr=2e-3):
+    """Train the learned CG initial guess on PPE snapshots of configs 0, 1 and
+    2 (the 2D dam, the 1.6 M-particle 3D dam in FP64 and in mixed precision),
+    the training set the two-phase configuration names.  One network: its
+    training state (weights, Adam moments and step count) passes from
+    context to context; each round takes per_round[k] snapshots of config k
+    (the defaults: config 0's whole 2000-step run and the first 100 steps of
+    configs 1 and 2, 2,200 snapshots).  Each snapshot is one solver step
+    (previous-pressure start) followed by `iters` Adam steps on the relative
+    residual the network's guess leaves in that step's system.  Not part of
+    any timed region; its cost is reported."""
+    import time
+    ctxs = []
+    for k in (0, 1, 2):
+        c, case, _ = build_case(0, k)
+        s = vm.Solver(c, case, device=dev)
+        s.init()
+        s.gnn_create(GNN_LAYERS, 1)
+        ctxs.append(s)
+    state = ctxs[0].gnn_state()
+    P = len(ctxs[0].gnn_params())
+    losses = ([], [], [])
+    t0 = time.perf_counter()
+    for _ in range(rounds):
+        for k, s in enumerate(ctxs):
+            s.gnn_state(set_to=state)
+            for _ in range(per_round[k]):
+                s.step()
+                losses[k].append(s.gnn_train(iters, lr, objective="residual"))
+            state = s.gnn_state()
+    sec = time.perf_counter() - t0
+    for s in ctxs:
+        s.close()
+
+    def ends(v):
+        k = max(1, min(10, len(v) // 4))
+        return float(sum(v[:k]) / k), float(sum(v[-k:]) / k)
+    return {"params": state[:P],
+            "info": {"source": "PPE snapshots of configs 0, 1 and 2",
+                     "snapshots": {f"config{k}": rounds * per_round[k] for k in range(3)},
+                     "adam_steps_per_snapshot": iters, "lr": lr,
+                     "objective": "|b - A x0|^2 / |b|^2 of the guess x0",
+                     "loss_first_last": {f"config{k}": ends(losses[k]) for k in range(3)},
+                     "seconds": sec,
+                     "network": "4 residual message-passing layers, width 64, BF16 weights "
+                                "and activations, FP32 sums"}}
+
+
+def compare_guesses(vm, cfg, case, scenes, dev, params, args, steps=20, own=None):
     """CG iterations, initial relative residual and step time for the zero,
     previous-pressure and learned starting points, each in a fresh context
     advanced past the training steps, then timed over `steps` steps (graph
     mode, CUDA events)."""
     import torch
     out = {}
-    for name in ("zero", "previous", "extrapolated", "learned"):
+    names = ["zero", "previous", "extrapolated", "learned"] + (["learned_own_scene"] if own is not None
+                                                               else [])
+    for name in names:
         c = dict(cfg)
         c["warm_start"] = {"zero": 0, "extrapolated": 2}.get(name, 1)
         s = vm.Solver(c, case, device=dev)
         if scenes is not None:
             s.set_scenes(*scenes)
         s.init()
-        if name == "learned":
+        if name.startswith("learned"):
             s.gnn_create(GNN_LAYERS, 0)
-            s.gnn_params(set_to=params)
+            s.gnn_params(set_to=params if name == "learned" else own)
             s.gnn_use(True)
         s.set_graph(bool(args.graph))
         for _ in range(args.gnn_train_steps + max(args.warmup, 3)):
@@ -673,6 +732,9 @@ def main():
                     help="1: pick launch shapes by timing candidates on the first steps")
     ap.add_argument("--guess", default=None, choices=["zero", "previous", "extrapolated", "learned"],
                     help="CG starting point (default: learned for configs 3 and 4)")
+    ap.add_argument("--guess-train", default=None, choices=["configs", "own"],
+                    help="training snapshots of the learned guess: configs 0-2 (the default "
+                         "for config 3, which names them) or the benchmark scene's own")
     ap.add_argument("--gnn-train-steps", type=int, default=300,
                     help="solver steps of online training for the learned guess")
     ap.add_argument("--precision", type=int, default=None, choices=[0, 1, 2],

@@ -235,6 +235,10 @@ int mps_gnn_use(mps_ctx* ctx, int on);
 int mps_gnn_train(mps_ctx* ctx, int iters, float lr, int objective, int grad_only, float* loss);
 /* copy the FP32 parameters out (get) and/or in (set, resets Adam); *count = P */
 int mps_gnn_params(mps_ctx* ctx, float* get, const float* set, int* count);
+/* the whole training state out and/or in: parameters, Adam's first and
+ * second moments (P each) and its step count; *count = 3P + 1.  Passing it
+ * from context to context trains one network on several scenes. */
+int mps_gnn_state(mps_ctx* ctx, float* get, const float* set, int* count);
 /* inputs of the current state / forward pass on the captured inputs */
 int mps_gnn_features(mps_ctx* ctx);
 int mps_gnn_forward(mps_ctx* ctx);

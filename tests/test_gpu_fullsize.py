@@ -8,7 +8,9 @@ tests/test_oracle_pin.py) at the benchmark sizes (needs a B200):
 
 each at the initial lattice and again after 20 GPU steps, when particles
 have left the lattice: the lists are rebuilt at the GPU's own positions
-(mps_neighbors) and the oracle bins the same positions.
+(mps_neighbors) and the oracle bins the same positions.  Along long runs
+too: the 2D dam over its whole 2000 steps and a small 3D dam over 600, at
+the splashing states the collapse produces.
 """
 import numpy as np
 import pytest
@@ -64,3 +66,28 @@ def test_batched_64_scenes_lists_bit_exact():
     base, scenes = config.baseline(4)
     cfg, case, sid, boxes, pmax = config.batched(gpu_cfg(base, precision=1), scenes)
     run_case(cfg, case, scenes=(sid, boxes, pmax))
+
+
+def run_long(cfg, case, steps, every):
+    """Lists against the oracle's NEIGHBOR along a long run, while the flow
+    splashes and particles pack irregularly (the x-windows of the list
+    passes see every spacing the run produces)."""
+    g = vm.Solver(cfg, case)
+    assert g.init() == 0
+    g.set_graph(True)
+    for k in range(1, steps + 1):
+        assert g.step() == 0
+        if k % every == 0:
+            assert g.NEIGHBOR() == 0
+            check_lists(g, cfg, f"after {k} steps")
+    g.close()
+
+
+def test_dam2d_whole_run_lists_bit_exact():
+    cfg, case = config.baseline(0)
+    run_long(gpu_cfg(cfg), case, 2000, 250)
+
+
+def test_dam3d_small_long_run_lists_bit_exact():
+    cfg, case = config.scaled_dam3d(1)
+    run_long(gpu_cfg(cfg), case, 600, 100)

@@ -169,3 +169,30 @@ def test_learned_guess_graph_matches_eager():
     for f in out[0][0]:
         assert np.array_equal(out[0][0][f], out[1][0][f]), f
     assert out[0][1] == out[1][1]
+
+
+def test_training_state_moves_between_contexts():
+    """mps_gnn_state carries weights, Adam moments and the step count: a
+    network trained in one context and continued in another takes exactly
+    the Adam steps it would have taken in the first (same snapshot, same
+    state), and a state round trip is exact."""
+    a, b = _ctx(steps=2), _ctx(steps=2)
+    a.gnn_train(3, 1e-3)
+    st = a.gnn_state()
+    P = a.gnn_params().size
+    assert st.size == 3 * P + 1 and st[3 * P] == 3.0
+    assert np.any(st[P:2 * P] != 0) and np.any(st[2 * P:3 * P] != 0)
+    b.gnn_state(set_to=st)
+    assert np.array_equal(b.gnn_state(), st)
+    assert np.array_equal(b.gnn_params(), a.gnn_params())
+    # both contexts hold the same snapshot (same case, same steps): two more
+    # Adam steps from the same state give the same weights
+    a.gnn_train(2, 1e-3)
+    b.gnn_train(2, 1e-3)
+    assert np.array_equal(a.gnn_params(), b.gnn_params())
+    assert a.gnn_state()[3 * P] == 5.0
+    # setting the parameters alone restarts Adam
+    b.gnn_params(set_to=a.gnn_params())
+    assert b.gnn_state()[3 * P] == 0.0
+    a.close()
+    b.close()

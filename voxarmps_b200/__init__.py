@@ -46,7 +46,8 @@ EXPORTS = [
     "mps_write_vtu", "mps_stream", "mps_set_state", "mps_get_state", "mps_set_field",
     "mps_set_profile",
     "mps_cell_order_noalloc", "mps_set_scenes", "mps_set_graph",
-    "mps_gnn_create", "mps_gnn_use", "mps_gnn_train", "mps_gnn_params", "mps_gnn_features",
+    "mps_gnn_create", "mps_gnn_use", "mps_gnn_train", "mps_gnn_params", "mps_gnn_state",
+    "mps_gnn_features",
     "mps_gnn_forward", "mps_gnn_download", "mps_get_tuning", "mps_set_tuning", "mps_autotune",
     "mps_snapshot_vtu", "mps_wait_io", "mps_save_checkpoint", "mps_load_checkpoint",
     "mps_set_owned", "mps_set_n0", "mps_get_rows", "mps_set_rows", "mps_ppe_assemble",
@@ -114,6 +115,7 @@ def load_library(path: str = LIB_PATH):
     lib.mps_gnn_use.argtypes = [P, C.c_int]
     lib.mps_gnn_train.argtypes = [P, C.c_int, C.c_float, C.c_int, C.c_int, FP]
     lib.mps_gnn_params.argtypes = [P, FP, FP, C.POINTER(C.c_int)]
+    lib.mps_gnn_state.argtypes = [P, FP, FP, C.POINTER(C.c_int)]
     lib.mps_gnn_features.argtypes = [P]
     lib.mps_gnn_forward.argtypes = [P]
     lib.mps_gnn_download.argtypes = [P, C.c_char_p, P, C.POINTER(C.c_long)]
@@ -396,6 +398,21 @@ class Solver:
             src = src.ctypes.data_as(C.POINTER(C.c_float))
         self._chk(self.lib.mps_gnn_params(self.h, out.ctypes.data_as(C.POINTER(C.c_float)), src,
                                           None), "gnn_params")
+        return out
+
+    def gnn_state(self, set_to=None) -> np.ndarray:
+        """The training state (parameters, Adam moments, Adam step count);
+        with set_to, load one taken from another context first."""
+        cnt = C.c_int()
+        self._chk(self.lib.mps_gnn_state(self.h, None, None, C.byref(cnt)), "gnn_state")
+        out = np.zeros(cnt.value, np.float32)
+        src = None
+        if set_to is not None:
+            src = np.ascontiguousarray(set_to, np.float32)
+            assert src.size == cnt.value
+            src = src.ctypes.data_as(C.POINTER(C.c_float))
+        self._chk(self.lib.mps_gnn_state(self.h, out.ctypes.data_as(C.POINTER(C.c_float)), src,
+                                         None), "gnn_state")
         return out
 
     def gnn_features(self):

@@ -266,6 +266,9 @@ int allocate(mps_ctx* c)
                        &c->moff};
     for (auto f : ifields) TRY(dalloc(c, f, P));
     TRY(dalloc(c, &c->S6, 6 * P));
+    TRY(dalloc(c, &c->bx_l, P));
+    TRY(dalloc(c, &c->bx_s, P));
+    TRY(dalloc(c, &c->key_s, P));
     TRY(dalloc(c, &c->stage_in, P));
     TRY(dalloc(c, &c->P4, P));
     TRY(dalloc(c, &c->P4s, P));
@@ -1000,9 +1003,27 @@ int mps_download(mps_ctx* c, const char* field, void* out, long* count)
         k_unpermute_i<<<grid_blocks(n), kBlock, 0, st>>>(n, c->oid, a, istage);
         VMPS_CUDA(c, cudaMemcpyAsync(out, istage, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
     } else if (f == "perm_l" || f == "perm_s") {
-        k_perm_ids<<<grid_blocks(n), kBlock, 0, st>>>(n, c->oid, f == "perm_s" ? c->perm_s : nullptr,
-                                                       istage);
-        VMPS_CUDA(c, cudaMemcpyAsync(out, istage, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+        // the context orders a cell's particles by (x, id); NEIGHBOR's
+        // permutations by id alone (functions.cu:2820): ids and cells in
+        // the grid's order, then each cell's run sorted
+        const bool pnd = f == "perm_s";
+        std::vector<int> cl(n);
+        int* o = (int*)out;
+        k_perm_ids<<<grid_blocks(n), kBlock, 0, st>>>(n, c->oid, pnd ? c->perm_s : nullptr, istage);
+        k_perm_ids<<<grid_blocks(n), kBlock, 0, st>>>(n, pnd ? c->cell_s : c->cell_l,
+                                                       pnd ? c->perm_s : nullptr, istage + n);
+        vmps_count_launch(2);
+        VMPS_CUDA(c, cudaMemcpyAsync(o, istage, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+        VMPS_CUDA(c, cudaMemcpyAsync(cl.data(), istage + n, sizeof(int) * n,
+                                     cudaMemcpyDeviceToHost, st));
+        VMPS_CUDA(c, cudaStreamSynchronize(st));
+        for (int a = 0; a < n;) {
+            int b = a + 1;
+            while (b < n && cl[b] == cl[a]) b++;
+            std::sort(o + a, o + b);
+            a = b;
+        }
+        return MPS_OK;
     } else {
         c->msg = "unknown field " + f;
         return MPS_ERR_ARG;

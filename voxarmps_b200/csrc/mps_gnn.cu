@@ -1334,6 +1334,45 @@ int mps_gnn_params(mps_ctx* c, float* get, const float* set, int* count)
     return MPS_OK;
 }
 
+// The whole training state: FP32 parameters, Adam's two moments and its step
+// count (as a float), 3P + 1 values.  Moving it between contexts trains one
+// network on several scenes' PPE snapshots with one Adam trajectory.
+int mps_gnn_state(mps_ctx* c, float* get, const float* set, int* count)
+{
+    if (!c || !c->gnn) return MPS_ERR_ARG;
+    vmps_gnn* G = c->gnn;
+    const int P = G->lay.P;
+    if (count) *count = 3 * P + 1;
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    if (set) {
+        const double t = set[3 * P];
+        if (!(t >= 0.0 && t < 1e15)) {
+            c->msg = "network state: bad Adam step count";
+            return MPS_ERR_ARG;
+        }
+        VMPS_CUDA(c, cudaMemcpyAsync(G->w, set, sizeof(float) * P, cudaMemcpyHostToDevice,
+                                     c->stream));
+        VMPS_CUDA(c, cudaMemcpyAsync(G->m, set + P, sizeof(float) * P, cudaMemcpyHostToDevice,
+                                     c->stream));
+        VMPS_CUDA(c, cudaMemcpyAsync(G->v, set + 2 * P, sizeof(float) * P,
+                                     cudaMemcpyHostToDevice, c->stream));
+        k_gnn_to16<<<(P + kThreads - 1) / kThreads, kThreads, 0, c->stream>>>(P, G->w, G->w16);
+        vmps_count_launch(1);
+        G->t = (long)t;
+    }
+    if (get) {
+        VMPS_CUDA(c, cudaMemcpyAsync(get, G->w, sizeof(float) * P, cudaMemcpyDeviceToHost,
+                                     c->stream));
+        VMPS_CUDA(c, cudaMemcpyAsync(get + P, G->m, sizeof(float) * P, cudaMemcpyDeviceToHost,
+                                     c->stream));
+        VMPS_CUDA(c, cudaMemcpyAsync(get + 2 * P, G->v, sizeof(float) * P,
+                                     cudaMemcpyDeviceToHost, c->stream));
+    }
+    VMPS_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (get) get[3 * P] = (float)G->t;
+    return MPS_OK;
+}
+
 // Features of the current state (as the next PPE would see them: call after
 // mps_step has produced n* and bcon, i.e. for the step just taken they are
 // the ones captured inside it).  Exposed for tests and offline training.

@@ -2,8 +2,9 @@
 // solver's translation units.
 //
 // Layout in HBM: structure-of-arrays, particles in cell order (re-sorted
-// every step by (cell, original id), the order NEIGHBOR's counting sort
-// produces, functions.cu:2820-2852).  Neighbour lists and the PPE matrix are
+// every step by (Laplacian-grid cell, x, original id); NEIGHBOR's counting
+// sort, functions.cu:2820-2852, orders a cell by id alone, and that order is
+// formed when the permutation is downloaded).  Neighbour lists and the PPE matrix are
 // row-major with a fixed row capacity: entry k of row i lives at i*cap + k.
 // Kernels over the Laplacian-radius list (about 300 entries per row in 3D)
 // give each row a whole warp; kernels over the PND-radius list (about 50)
@@ -206,6 +207,9 @@ struct mps_ctx {
     int *cnt_l = nullptr, *cst_l = nullptr;        // per cell count / start
     int *cnt_s = nullptr, *cst_s = nullptr;
     int *bslot_l = nullptr, *boid_l = nullptr;     // bucketed slots / ids
+    unsigned long long* bx_l = nullptr;            // order keys of x, bucketed (primary grid)
+    unsigned long long* bx_s = nullptr;            // the same on the PND grid
+    unsigned long long* key_s = nullptr;           // order keys of x in the PND grid's order
     int *bslot_s = nullptr, *boid_s = nullptr;
     int *src = nullptr, *inv = nullptr;            // new slot <- old slot, old -> new
     int *perm_s = nullptr, *perm_s_tmp = nullptr;  // small-grid cell order (slots)

@@ -8,13 +8,18 @@
 //                  bucket counts by atomics;
 //   2. scan        exclusive prefix sums of the counts (cell starts);
 //   3. k_scatter   particles into their cell bucket (arbitrary order);
-//   4. k_rank      order inside a bucket by original id: the stable counting
+//   4. k_rank      order inside a bucket: by (x, original id) on the
+//                  Laplacian grid, so that every x-triple of cells is sorted
+//                  by x; by original id on the PND grid, the stable counting
 //                  sort of the reference's insertion loop (functions.cu:2820);
+//                  NEIGHBOR's own Laplacian-grid order is formed on download;
 //   5. k_gather    reorder the persistent particle state into cell order;
-//   6. k_lists     both lists in the reference's scan order (row, colu, dep;
-//                  ascending id inside a cell), membership decided with the
-//                  reference's exact FP64 arithmetic; a warp per particle for
-//                  the Laplacian radius, GS lanes for the PND radius.
+//   6. k_lists     both lists, membership decided with the reference's exact
+//                  FP64 arithmetic; Q particles of one cell per warp for the
+//                  Laplacian radius (x-windowed runs), GS lanes per particle
+//                  for the PND radius.  Exported rows are put back in the
+//                  reference's scan order (x offset outermost, then y, z;
+//                  ascending id inside a cell).
 #include <cmath>
 #include <cstdio>
 
@@ -123,12 +128,23 @@ __global__ void k_scan_apply(int m, const int* __restrict__ in, const int* __res
     }
 }
 
+// Unsigned key whose integer order is the order of the doubles (-0 just
+// below +0, NaNs at the ends), so that (key, id) is a strict total order
+// even on a state that has gone non-finite: every bucket position is taken
+// exactly once.
+__device__ __forceinline__ unsigned long long order_key(double v)
+{
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
 __global__ void k_scatter(int n, const int* __restrict__ cell_l, const int* __restrict__ cell_s,
                           const int* __restrict__ bpos_l, const int* __restrict__ bpos_s,
                           const int* __restrict__ cst_l, const int* __restrict__ cst_s,
-                          const int* __restrict__ oid, int* __restrict__ bslot_l,
-                          int* __restrict__ boid_l, int* __restrict__ bslot_s,
-                          int* __restrict__ boid_s)
+                          const int* __restrict__ oid, const double* __restrict__ x,
+                          int* __restrict__ bslot_l, int* __restrict__ boid_l,
+                          unsigned long long* __restrict__ bx_l, int* __restrict__ bslot_s,
+                          int* __restrict__ boid_s, unsigned long long* __restrict__ bx_s)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -136,36 +152,57 @@ __global__ void k_scatter(int n, const int* __restrict__ cell_l, const int* __re
     int q = cst_l[cell_l[i]] + bpos_l[i];
     bslot_l[q] = i;
     boid_l[q] = o;
+    const unsigned long long key = order_key(x[i]);
+    bx_l[q] = key;
     int qs = cst_s[cell_s[i]] + bpos_s[i];
     bslot_s[qs] = i;
     boid_s[qs] = o;
+    bx_s[qs] = key;
 }
 
-// Rank inside the bucket by original id.  Primary grid: src[new] = old slot
-// and inv[old] = new.  PND grid: perm_tmp[position] = old slot.
+// Rank inside the bucket by (x, original id) on both grids, so that every
+// cell's particles lie in ascending x and each x-triple of cells is sorted
+// by x (the list passes window their candidate runs on x).  Laplacian grid
+// (the memory order): src[new] = old slot and inv[old] = new.  PND grid:
+// perm_tmp[position] = old slot and key_s[position] = x's order key.
+// NEIGHBOR's own orders, (cell, id) on each grid (the stable counting sort
+// of the reference's insertion loop, functions.cu:2820), are formed when
+// the permutations are downloaded.
 __global__ void k_rank(int n, const int* __restrict__ cell_l, const int* __restrict__ cell_s,
                        const int* __restrict__ cst_l, const int* __restrict__ cnt_l,
                        const int* __restrict__ cst_s, const int* __restrict__ cnt_s,
                        const int* __restrict__ bslot_l, const int* __restrict__ boid_l,
+                       const unsigned long long* __restrict__ bx_l,
                        const int* __restrict__ bslot_s, const int* __restrict__ boid_s,
-                       int* __restrict__ src, int* __restrict__ inv, int* __restrict__ perm_tmp)
+                       const unsigned long long* __restrict__ bx_s,
+                       int* __restrict__ src, int* __restrict__ inv, int* __restrict__ perm_tmp,
+                       unsigned long long* __restrict__ key_s)
 {
     int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) return;
     {
         int s = bslot_l[q], me = boid_l[q];
+        const unsigned long long xm = bx_l[q];
         int c = cell_l[s];
         int b = cst_l[c], e = b + cnt_l[c], r = 0;
-        for (int t = b; t < e; t++) r += (boid_l[t] < me);
+        for (int t = b; t < e; t++) {
+            const unsigned long long xt = bx_l[t];
+            r += (xt < xm || (xt == xm && boid_l[t] < me));
+        }
         src[b + r] = s;
         inv[s] = b + r;
     }
     {
         int s = bslot_s[q], me = boid_s[q];
+        const unsigned long long xm = bx_s[q];
         int c = cell_s[s];
         int b = cst_s[c], e = b + cnt_s[c], r = 0;
-        for (int t = b; t < e; t++) r += (boid_s[t] < me);
+        for (int t = b; t < e; t++) {
+            const unsigned long long xt = bx_s[t];
+            r += (xt < xm || (xt == xm && boid_s[t] < me));
+        }
         perm_tmp[b + r] = s;
+        key_s[b + r] = xm;
     }
 }
 
@@ -216,13 +253,17 @@ __global__ void k_translate(int n, const int* __restrict__ inv, const int* __res
 // One list, G lanes per particle, row-major.  Membership is the reference's
 // exact FP64 rule (3D: d <= cut, self included; 2D: d < cut, self excluded)
 // over the 3x3(x3) cells around the particle's cell (functions.cu:2854-2918).
-// The three cells of one (y, z) offset are consecutive in memory (cells are
-// numbered x fastest and particles are stored in cell order), so they are
-// scanned as one range; cells whose box lies farther than the cutoff from
-// the particle are left out of the range (conservative margin).  Rows are
-// stored in scan order (y, z outer, memory order inside); the reference's
-// own order (x offset outermost, ascending id per cell) is restored when
-// lists are exported (mps_download_lists).
+// The three cells of one (y, z) offset are consecutive in the grid's order
+// (cells are numbered x fastest), so they are scanned as one range; cells
+// whose box lies farther than the cutoff from the particle are left out.
+// Inside a cell the order is by x, so a range is sorted by x and shrinks to
+// the x-window [x_i - r, x_i + r], r the largest |dx| that the particle's
+// distance to the range's (y, z) cells leaves under the cutoff
+// (conservative margins); the lanes of the group find the windows of their
+// runs (lane l: runs l, l + G, ...) by binary searches over the order keys
+// of x.  Rows are stored in scan order (y, z outer, memory order inside);
+// the reference's own order (x offset outermost, ascending id per cell) is
+// restored when lists are exported (mps_download_lists).
 // 8 resident blocks per SM (32 registers, a few bytes of spills in 3D):
 // the PND-radius list stage 0.16 ms faster than at 48 registers on the
 // 1.6 M-particle dam (6 blocks: 0.08 ms; the Laplacian list's k_lists_q
@@ -232,6 +273,7 @@ __global__ void __launch_bounds__(256, 8) k_lists(int n, Grid g, double cut, flo
                         const double4* __restrict__ P4, const float4* __restrict__ P4f,
                         const int* __restrict__ cell, const int* __restrict__ cst,
                         const int* __restrict__ cnt, const int* __restrict__ perm,
+                        const unsigned long long* __restrict__ keys,
                         int* __restrict__ out, int* __restrict__ len, int* len_max, int which,
                         unsigned int* err)
 {
@@ -261,45 +303,73 @@ __global__ void __launch_bounds__(256, 8) k_lists(int n, Grid g, double cut, flo
         return d > 0 ? d * d : 0.0;
     };
     const double gxl = gap2(-1, lox, hix), gxh = gap2(1, lox, hix);
+    const int ndp = m6 - m5 + 1, nt = (m4 - m3 + 1) * ndp;
+    // the windows of this lane's runs t = lane, lane + G, ...
+    constexpr int R = ((DIM == 3 ? 9 : 3) + G - 1) / G;
+    int wb[R], we[R];
+#pragma unroll
+    for (int u = 0; u < R; u++) {
+        const int t = q.lane + u * G;
+        wb[u] = 0;
+        we[u] = 0;
+        if (t >= nt) continue;
+        const int cu = m3 + t / ndp, dp = m5 + t % ndp;
+        const double gyz = gap2(cu, loy, hiy) + (DIM == 3 ? gap2(dp, loz, hiz) : 0.0);
+        if (gyz > cut) continue;
+        const int rlo = (m1 < 0 && gyz + gxl <= cut) ? -1 : 0;
+        const int rhi = (m2 > 0 && gyz + gxh <= cut) ? 1 : 0;
+        const int Cr = ic + (jc - 1 + cu) * g.ncx + (kc - 1 + dp) * g.ncx * g.ncy;
+        // |dx| above r puts the pair beyond the cutoff with room for every
+        // rounding of the distance
+        const double r = sqrt(cut - gyz) * (1.0 + 1e-12) + mx;
+        const unsigned long long klo = order_key(pi.x - r), khi = order_key(pi.x + r);
+        int lo_a = cst[Cr + rlo], hi_a = cst[Cr + rhi] + cnt[Cr + rhi];
+        int lo_b = lo_a, hi_b = hi_a;
+        while (lo_a < hi_a || lo_b < hi_b) {
+            const int ma = (lo_a + hi_a) >> 1, mb = (lo_b + hi_b) >> 1;
+            const bool sa = lo_a < hi_a, sb = lo_b < hi_b;
+            const unsigned long long va = sa ? keys[ma] : 0ull, vb = sb ? keys[mb] : 0ull;
+            if (sa) { if (va < klo) lo_a = ma + 1; else hi_a = ma; }
+            if (sb) { if (vb <= khi) lo_b = mb + 1; else hi_b = mb; }
+        }
+        wb[u] = lo_a;
+        we[u] = max(lo_a, lo_b);
+    }
     int* row = out + (size_t)i * cap;
     int k = 0;
-    for (int cu = m3; cu <= m4; cu++) {
-        double gy = gap2(cu, loy, hiy);
-        for (int dp = m5; dp <= m6; dp++) {
-            double gyz = gy + (DIM == 3 ? gap2(dp, loz, hiz) : 0.0);
-            if (gyz > cut) continue;
-            int rlo = (m1 < 0 && gyz + gxl <= cut) ? -1 : 0;
-            int rhi = (m2 > 0 && gyz + gxh <= cut) ? 1 : 0;
-            int Cr = ic + (jc - 1 + cu) * g.ncx + (kc - 1 + dp) * g.ncx * g.ncy;
-            int b = cst[Cr + rlo], e = cst[Cr + rhi] + cnt[Cr + rhi];
-            for (int base = b; base < e; base += G) {
-                int jj = base + q.lane;
-                bool in = false;
-                int j = 0;
-                if (jj < e) {
-                    j = perm ? perm[jj] : jj;
-                    // FP32 screen; the exact FP64 rule decides only inside
-                    // the screening margin [cut_lo, cut_hi]
-                    float4 fj = P4f[j];
-                    float ex = fj.x - fi.x, ey = fj.y - fi.y, ez = DIM == 3 ? fj.z - fi.z : 0.f;
-                    // fused multiply-adds: fewer roundings than the bound assumes
-                    float f2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
-                    if (f2 < cut_lo) {
-                        in = (DIM == 3) || (j != i);
-                    } else if (f2 <= cut_hi) {
-                        double4 pj = P4[j];
-                        double d2 = dist2<DIM>(pj.x - pi.x, pj.y - pi.y,
-                                               DIM == 3 ? pj.z - pi.z : 0.0);
-                        in = (DIM == 3) ? (d2 <= cut) : (j != i && d2 < cut);
-                    }
+#pragma unroll
+    for (int t = 0; t < (DIM == 3 ? 9 : 3); t++) {
+        if (t >= nt) break;
+        const int src_lane = (int)q.base + t % G;
+        const int b = __shfl_sync(q.mask, wb[t / G], src_lane);
+        const int e = __shfl_sync(q.mask, we[t / G], src_lane);
+        for (int base = b; base < e; base += G) {
+            int jj = base + q.lane;
+            bool in = false;
+            int j = 0;
+            if (jj < e) {
+                j = perm[jj];
+                // FP32 screen; the exact FP64 rule decides only inside
+                // the screening margin [cut_lo, cut_hi]
+                float4 fj = P4f[j];
+                float ex = fj.x - fi.x, ey = fj.y - fi.y, ez = DIM == 3 ? fj.z - fi.z : 0.f;
+                // fused multiply-adds: fewer roundings than the bound assumes
+                float f2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
+                if (f2 < cut_lo) {
+                    in = (DIM == 3) || (j != i);
+                } else if (f2 <= cut_hi) {
+                    double4 pj = P4[j];
+                    double d2 = dist2<DIM>(pj.x - pi.x, pj.y - pi.y,
+                                           DIM == 3 ? pj.z - pi.z : 0.0);
+                    in = (DIM == 3) ? (d2 <= cut) : (j != i && d2 < cut);
                 }
-                unsigned m = q.ballot(in);
-                if (in) {
-                    int pos = k + __popc(m & ((1u << q.lane) - 1u));
-                    if (pos < cap) row[pos] = j;
-                }
-                k += __popc(m);
             }
+            unsigned m = q.ballot(in);
+            if (in) {
+                int pos = k + __popc(m & ((1u << q.lane) - 1u));
+                if (pos < cap) row[pos] = j;
+            }
+            k += __popc(m);
         }
     }
     if (q.lane == 0) {
@@ -314,17 +384,23 @@ __global__ void __launch_bounds__(256, 8) k_lists(int n, Grid g, double cut, flo
 
 // The same lists for Q particles of one cell at a time, one warp: each
 // candidate's packed position is loaded once and tested against the Q
-// particles, so the load, the loop and the index work are shared.  The
-// scanned ranges are the union of the Q particles' culled ranges; a range
-// a particle would have culled holds none of its neighbours, so every row
-// receives exactly the entries, in exactly the order, of the one-particle
-// kernel above.  Groups whose particles sit in different cells are done
-// one particle at a time.
+// particles, so the load, the loop and the index work are shared.  Inside a
+// cell particles are ordered by x, so each (y, z) run of three cells is
+// sorted by x, and a run's candidates for the Q particles lie in one
+// contiguous x-window: [min_q(x_q - r_q), max_q(x_q + r_q)], r_q the largest
+// |dx| that the particle's distance to the run's (y, z) cells leaves under
+// the cutoff (conservative margin).  Lane t finds run t's window by two
+// interleaved binary searches over x.  Members keep their memory order, and
+// a window a particle's neighbours cannot lie outside of drops only
+// non-members, so every row receives exactly the entries, in exactly the
+// order, of the one-particle scan of the whole run.  Groups whose particles
+// sit in different cells are done one particle at a time.
 template <int DIM, int Q>
 __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const Grid& g,
                                           double cut, float cut_lo, float cut_hi, int cap,
                                           const double4* __restrict__ P4,
                                           const float4* __restrict__ P4f,
+                                          const double* __restrict__ xs,
                                           const int* __restrict__ cst, const int* __restrict__ cnt,
                                           int* __restrict__ out, int* __restrict__ len,
                                           int* len_max, int which, unsigned int* err)
@@ -340,9 +416,12 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
         double d = off < 0 ? lo : (off > 0 ? hi : 0.0);
         return d > 0 ? d * d : 0.0;
     };
-    // union of the particles' culling decisions per (y, z) offset t:
-    // scan t unless every particle culls it; widen to x-1 / x+1 if any wants
-    unsigned scan_t = 0, lo_t = 0, hi_t = 0;
+    // lane t < nt owns (y, z) run t: whether any particle needs it, whether
+    // any needs its x-1 / x+1 cell, and the union of their x-windows
+    const int ndp = m6 - m5 + 1, nt = (m4 - m3 + 1) * ndp;
+    const int cu = m3 + lane / ndp, dp = m5 + lane % ndp;
+    bool scan_me = false, lo_me = false, hi_me = false;
+    double xlo = INFINITY, xhi = -INFINITY;
     unsigned lt_mask;  // lanes below this one
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt_mask));
     float4 fi[Q];
@@ -353,28 +432,28 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
         if (q >= nq) continue;
         const double4 pi = P4[i0 + q];
         fi[q] = P4f[i0 + q];
+        if (lane >= nt) continue;
         const double lox = pi.x - (g.xmin + (ic - 1) * g.re) - mx;
         const double hix = (g.xmin + ic * g.re) - pi.x - mx;
         const double loy = pi.y - (g.ymin + (jc - 1) * g.re) - mx;
         const double hiy = (g.ymin + jc * g.re) - pi.y - mx;
-        double loz = 0, hiz = 0;
+        double gyz = gap2(cu, loy, hiy);
         if (DIM == 3) {
-            loz = pi.z - (g.zmin + (kc - 1) * g.rez) - mz;
-            hiz = (g.zmin + kc * g.rez) - pi.z - mz;
+            const double loz = pi.z - (g.zmin + (kc - 1) * g.rez) - mz;
+            const double hiz = (g.zmin + kc * g.rez) - pi.z - mz;
+            gyz += gap2(dp, loz, hiz);
         }
-        const double gxl = gap2(-1, lox, hix), gxh = gap2(1, lox, hix);
-        int t = 0;
-        for (int cu = m3; cu <= m4; cu++) {
-            const double gy = gap2(cu, loy, hiy);
-            for (int dp = m5; dp <= m6; dp++, t++) {
-                const double gyz = gy + (DIM == 3 ? gap2(dp, loz, hiz) : 0.0);
-                if (gyz > cut) continue;
-                scan_t |= 1u << t;
-                if (m1 < 0 && gyz + gxl <= cut) lo_t |= 1u << t;
-                if (m2 > 0 && gyz + gxh <= cut) hi_t |= 1u << t;
-            }
-        }
+        if (gyz > cut) continue;
+        scan_me = true;
+        if (m1 < 0 && gyz + gap2(-1, lox, hix) <= cut) lo_me = true;
+        if (m2 > 0 && gyz + gap2(1, lox, hix) <= cut) hi_me = true;
+        // |dx| above r puts the pair beyond the cutoff with room for every
+        // rounding of the distance
+        const double r = sqrt(cut - gyz) * (1.0 + 1e-12) + mx;
+        xlo = fmin(xlo, pi.x - r);
+        xhi = fmax(xhi, pi.x + r);
     }
+    const unsigned scan_t = __ballot_sync(0xffffffffu, scan_me);
     // one batch of 32 candidates against the Q particles
     auto batch = [&](int j, bool valid, float4 fj) {
 #pragma unroll
@@ -412,17 +491,24 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
             batch(j, valid, valid ? P4f[j] : make_float4(0.f, 0.f, 0.f, 0.f));
         }
     };
-    // the candidate range of every scanned (y, z) run, loaded at once (lane t
-    // holds run t's [b, e)) instead of one dependent load pair per run: the
-    // Laplacian list 0.11 ms faster on the 1.6 M-particle dam
-    const int ndp = m6 - m5 + 1, nt = (m4 - m3 + 1) * ndp;
+    // the candidate window of every scanned (y, z) run, found at once (lane
+    // t holds run t's [b, e)): first position with x >= xlo, first with
+    // x > xhi, both searches advancing together
     int rb = 0, rend = 0;
-    if (lane < nt && (scan_t >> lane & 1u)) {
-        const int cu = m3 + lane / ndp, dp = m5 + lane % ndp;
-        const int rlo = (lo_t >> lane & 1u) ? -1 : 0, rhi = (hi_t >> lane & 1u) ? 1 : 0;
+    if (scan_me) {
         const int Cr = ic + (jc - 1 + cu) * g.ncx + (kc - 1 + dp) * g.ncx * g.ncy;
-        rb = cst[Cr + rlo];
-        rend = cst[Cr + rhi] + cnt[Cr + rhi];
+        const int rlo = lo_me ? -1 : 0, rhi = hi_me ? 1 : 0;
+        const int b = cst[Cr + rlo], e = cst[Cr + rhi] + cnt[Cr + rhi];
+        int lo_a = b, hi_a = e, lo_b = b, hi_b = e;
+        while (lo_a < hi_a || lo_b < hi_b) {
+            const int ma = (lo_a + hi_a) >> 1, mb = (lo_b + hi_b) >> 1;
+            const bool sa = lo_a < hi_a, sb = lo_b < hi_b;
+            const double va = sa ? xs[ma] : 0.0, vb = sb ? xs[mb] : 0.0;
+            if (sa) { if (va < xlo) lo_a = ma + 1; else hi_a = ma; }
+            if (sb) { if (vb <= xhi) lo_b = mb + 1; else hi_b = mb; }
+        }
+        rb = lo_a;
+        rend = max(lo_a, lo_b);
     }
     for (int t = 0; t < nt; t++) {
         if (!(scan_t >> t & 1u)) continue;
@@ -448,6 +534,7 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
 template <int DIM, int Q>
 __global__ void __launch_bounds__(256, 4) k_lists_q(int n, Grid g, double cut, float cut_lo, float cut_hi, int cap,
                           const double4* __restrict__ P4, const float4* __restrict__ P4f,
+                          const double* __restrict__ xs,
                           const int* __restrict__ cell, const int* __restrict__ cst,
                           const int* __restrict__ cnt, int* __restrict__ out,
                           int* __restrict__ len, int* len_max, int which, unsigned int* err)
@@ -461,12 +548,12 @@ __global__ void __launch_bounds__(256, 4) k_lists_q(int n, Grid g, double cut, f
     bool same = true;
     for (int q = 1; q < nq; q++) same = same && cell[i0 + q] == C;
     if (same) {
-        list_rows<DIM, Q>(lane, i0, nq, C, g, cut, cut_lo, cut_hi, cap, P4, P4f, cst, cnt, out,
-                          len, len_max, which, err);
+        list_rows<DIM, Q>(lane, i0, nq, C, g, cut, cut_lo, cut_hi, cap, P4, P4f, xs, cst, cnt,
+                          out, len, len_max, which, err);
     } else {
         for (int q = 0; q < nq; q++)
             list_rows<DIM, Q>(lane, i0 + q, 1, cell[i0 + q], g, cut, cut_lo, cut_hi, cap, P4, P4f,
-                              cst, cnt, out, len, len_max, which, err);
+                              xs, cst, cnt, out, len, len_max, which, err);
     }
 }
 
@@ -557,11 +644,13 @@ int vmps_neighbors(mps_ctx* ctx)
     scan(ctx, ctx->gl.tnc + 2, ctx->cnt_l, ctx->cst_l, ctx->scan_tmp);
     scan(ctx, ctx->gs.tnc + 2, ctx->cnt_s, ctx->cst_s, ctx->scan_tmp);
     k_scatter<<<nb, kBlock, 0, st>>>(n, ctx->cell_l, ctx->cell_s, ctx->bpos_l, ctx->bpos_s,
-                                     ctx->cst_l, ctx->cst_s, ctx->oid, ctx->bslot_l, ctx->boid_l,
-                                     ctx->bslot_s, ctx->boid_s);
+                                     ctx->cst_l, ctx->cst_s, ctx->oid, ctx->x, ctx->bslot_l,
+                                     ctx->boid_l, ctx->bx_l, ctx->bslot_s, ctx->boid_s,
+                                     ctx->bx_s);
     k_rank<<<nb, kBlock, 0, st>>>(n, ctx->cell_l, ctx->cell_s, ctx->cst_l, ctx->cnt_l, ctx->cst_s,
-                                  ctx->cnt_s, ctx->bslot_l, ctx->boid_l, ctx->bslot_s,
-                                  ctx->boid_s, ctx->src, ctx->inv, ctx->perm_s_tmp);
+                                  ctx->cnt_s, ctx->bslot_l, ctx->boid_l, ctx->bx_l,
+                                  ctx->bslot_s, ctx->boid_s, ctx->bx_s, ctx->src, ctx->inv,
+                                  ctx->perm_s_tmp, ctx->key_s);
     vmps_count_launch(2);
     // reorder persistent state into cell order
     GatherSet g;
@@ -594,32 +683,32 @@ int vmps_neighbors(mps_ctx* ctx)
         if (ctx->cfg.dim == 3) {
             constexpr int GS = SmallG<3>::G;
             k_lists_q<3, kListQ><<<nq32, kBlock, 0, st>>>(
-                n, ctx->gl, ctx->cut_l, lo_l, hi_l, ctx->cap_l, ctx->P4, ctx->P4f, ctx->cell_l,
-                ctx->cst_l, ctx->cnt_l, ctx->nbr_l, ctx->len_l, ctx->len_max, 0, ctx->d_err);
+                n, ctx->gl, ctx->cut_l, lo_l, hi_l, ctx->cap_l, ctx->P4, ctx->P4f, ctx->x,
+                ctx->cell_l, ctx->cst_l, ctx->cnt_l, ctx->nbr_l, ctx->len_l, ctx->len_max, 0, ctx->d_err);
             if (ctx->tune_small_wide)
                 k_lists<3, 2 * GS><<<(int)(((long)n * 2 * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
                     n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,
-                    ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
+                    ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->key_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
                     ctx->d_err);
             else
                 k_lists<3, GS><<<(int)(((long)n * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
                     n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,
-                    ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
+                    ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->key_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
                     ctx->d_err);
         } else {
             constexpr int GS = SmallG<2>::G;
             k_lists_q<2, kListQ><<<nq32, kBlock, 0, st>>>(
-                n, ctx->gl, ctx->cut_l, lo_l, hi_l, ctx->cap_l, ctx->P4, ctx->P4f, ctx->cell_l,
-                ctx->cst_l, ctx->cnt_l, ctx->nbr_l, ctx->len_l, ctx->len_max, 0, ctx->d_err);
+                n, ctx->gl, ctx->cut_l, lo_l, hi_l, ctx->cap_l, ctx->P4, ctx->P4f, ctx->x,
+                ctx->cell_l, ctx->cst_l, ctx->cnt_l, ctx->nbr_l, ctx->len_l, ctx->len_max, 0, ctx->d_err);
             if (ctx->tune_small_wide)
                 k_lists<2, 2 * GS><<<(int)(((long)n * 2 * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
                     n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,
-                    ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
+                    ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->key_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
                     ctx->d_err);
             else
                 k_lists<2, GS><<<(int)(((long)n * GS + kBlock - 1) / kBlock), kBlock, 0, st>>>(
                     n, ctx->gs, ctx->cut_s, lo_s, hi_s, ctx->cap_s, ctx->P4, ctx->P4f, ctx->cell_s,
-                    ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
+                    ctx->cst_s, ctx->cnt_s, ctx->perm_s, ctx->key_s, ctx->nbr_s, ctx->len_s, ctx->len_max, 1,
                     ctx->d_err);
         }
     }

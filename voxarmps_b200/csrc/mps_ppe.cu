@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
                            int2* __restrict__ mcv32, int* __restrict__ mlen,
                            double* __restrict__ diag, double* __restrict__ source, int w_bcon,
                            int2* __restrict__ mrow, const int* __restrict__ own,
-                           int* __restrict__ sysmask)
+                           int* __restrict__ sysmask, double* __restrict__ r0)
 {
     Grp<kAsmG> q;
     int i = (int)q.gid;
@@ -99,7 +99,9 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
             diag[i] = 0.0;
             source[i] = 0.0;
             if (warm == 2) pold[i] = pnew[i];
-            pnew[i] = 0.0;
+            // with r0 the rows read every neighbour's guess: CG's start
+            // zeroes this one instead
+            if (!r0) pnew[i] = 0.0;
         }
         return;
     }
@@ -116,15 +118,16 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
     const int* row = nbr + (size_t)i * cap;
     int* crow = mcol + moff[i];
     double* vrow = mval + moff[i];
-    double dg = 0.0;
+    double dg = 0.0, ax = 0.0;
     int cnt = 0, L = len[i];
     for (int base = 0; base < L; base += kAsmG) {
         int k = base + q.lane;
-        double v = 0.0;
+        double v = 0.0, xj = 0.0;
         int j = -1;
         bool keep = false;
         if (k < L) {
             j = row[k];
+            if (r0) xj = pnew[j];  // the initial guess, read beside the position
             double4 pj;
             int bj;
             if (w_bcon) {  // P4's w slot holds bcon: one gather
@@ -150,15 +153,20 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
             crow[pos] = j;
             vrow[pos] = -v;
             if (mcv32) mcv32[moff[i] + pos] = make_int2(j, __float_as_int((float)(-v)));
+            ax += (-v) * xj;
         }
         cnt += __popc(m);
     }
     dg = q.sum(dg);
+    if (r0) ax = q.sum(ax);
     if (q.lane == 0) {
         diag[i] = dg + A.reg;
         mlen[i] = cnt;
         mrow[i] = make_int2(moff[i], cnt);
         if (!A.srcopt) source[i] = 1.0 / A.dt / A.dt * (nsrc[i] - A.n0_s) / A.n0_s;
+        // CG's starting residual b - A x0 of this row, from the entries just
+        // formed (x0 = the previous pressure, which this pass leaves as is)
+        if (r0) r0[i] = source[i] - ((dg + A.reg) * pnew[i] + ax);
         // initial guess: 0, the previous pressure, or the linear extrapolation
         // 2 p^n - p^(n-1) (pold keeps p^n for the next step)
         if (!warm) {
@@ -333,6 +341,46 @@ __global__ void __launch_bounds__(256, 8) k_cg_start(CG A, const double* __restr
             zv[i] = zi;
             p[i] = zi;
         }
+    }
+    bb = block_sum(bb, sh);
+    rz = block_sum(rz, sh);
+    rr = block_sum(rr, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = bb;
+        part[A.nparts + blockIdx.x] = rz;
+        part[2 * A.nparts + blockIdx.x] = rr;
+    }
+}
+
+// The same start when the assembly has already formed r = b - A x0 (in r):
+// z = M^-1 r, p = z and the partials b.b, r.z, r.r, one thread per row; rows
+// outside the system get r = z = p = 0 and Dirichlet rows their pressure 0
+// (the assembly left the guess untouched for its neighbours to read).
+__global__ void __launch_bounds__(256, 8) k_cg_start_rows(CG A, const double* __restrict__ b,
+                                                          const int* __restrict__ bcon,
+                                                          double* __restrict__ x,
+                                                          double* __restrict__ r,
+                                                          double* __restrict__ zv,
+                                                          double* __restrict__ p,
+                                                          double* __restrict__ part)
+{
+    __shared__ double sh[33];
+    double bb = 0, rz = 0, rr = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+        double ri = 0, zi = 0;
+        if (A.bcon[i] == 0) {
+            const double bi = b[i];
+            ri = r[i];
+            zi = A.precond ? ri / A.diag[i] : ri;
+            bb += bi * bi;
+            rz += ri * zi;
+            rr += ri * ri;
+        } else {
+            r[i] = 0.0;
+            if (bcon[i] != 0) x[i] = 0.0;
+        }
+        zv[i] = zi;
+        p[i] = zi;
     }
     bb = block_sum(bb, sh);
     rz = block_sum(rz, sh);
@@ -808,7 +856,7 @@ int vmps_ppe_apply(mps_ctx* c, const double* x, double* y)
 // follows in vmps_ppe or, for a scene split between contexts, in the
 // host-driven CG entry points below.  *warm_out: the initial guess used
 // (0: zero, the start kernels then skip the product).
-static int ppe_assemble(mps_ctx* c, int* warm_out)
+static int ppe_assemble(mps_ctx* c, int* warm_out, double* r0 = nullptr, bool* fused = nullptr)
 {
     const mps_config& f = c->cfg;
     cudaStream_t st = c->stream;
@@ -840,6 +888,11 @@ static int ppe_assemble(mps_ctx* c, int* warm_out)
         int r = vmps_scan(c, n, c->len_l, c->moff);
         if (r != MPS_OK) return r;
     }
+    // CG's starting residual in the same pass: a guess the pass does not
+    // change (the previous pressure or the network's) and a source known
+    // per row (not the sequential HS + ECS recurrence)
+    if (fused) *fused = r0 && warm == 1 && !f.srcopt;
+    if (!fused || !*fused) r0 = nullptr;
     const int wblocks = (int)(((long)n * kAsmG + kBlock - 1) / kBlock);
     // the predicted positions carry bcon in their w slot when BCON ran after
     // the last PREDICTION (always within a step; the per-stage entry points
@@ -849,12 +902,12 @@ static int ppe_assemble(mps_ctx* c, int* warm_out)
         k_assemble<3><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
                                                   nsrc, warm, c->pnew, c->pold, c->moff, c->mcol,
                                                   c->mval, c->mcv32, c->mlen, c->diag, c->source,
-                                                  w_bcon, c->mrow, c->own, c->sysmask);
+                                                  w_bcon, c->mrow, c->own, c->sysmask, r0);
     else
         k_assemble<2><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
                                                   nsrc, warm, c->pnew, c->pold, c->moff, c->mcol,
                                                   c->mval, c->mcv32, c->mlen, c->diag, c->source,
-                                                  w_bcon, c->mrow, c->own, c->sysmask);
+                                                  w_bcon, c->mrow, c->own, c->sysmask, r0);
     vmps_count_launch(1);
     if (f.srcopt) {
         // slot of particle id k: inv_id[k] (the sort's inv buffer is free here)
@@ -897,9 +950,11 @@ int vmps_ppe(mps_ctx* c)
     const mps_config& f = c->cfg;
     cudaStream_t st = c->stream;
     const int n = c->n;
+    const bool mixed = f.precision >= 1;
     int warm = 0, nblk = 0;
+    bool fused = false;
     {
-        int r = ppe_assemble(c, &warm);
+        int r = ppe_assemble(c, &warm, mixed ? nullptr : c->cg_r, &fused);
         if (r != MPS_OK) return r;
         r = cg_grid(c, &nblk);
         if (r != MPS_OK) return r;
@@ -918,11 +973,15 @@ int vmps_ppe(mps_ctx* c)
     const bool graph = cap == cudaStreamCaptureStatusActive;
     cudaGraphConditionalHandle cond = 0;
     if (graph) VMPS_CUDA(c, cudaGraphConditionalHandleCreate(&cond, cgraph, 1, cudaGraphCondAssignDefault));
-    const bool mixed = f.precision >= 1;
     IR I{c->mcv32, c->ir_d, c->ir_r, c->ir_z, c->ir_p, c->ir_s};
     if (mixed) {
         k_ir_start<<<nblk, kRedThreads, 0, st>>>(G, I, c->source, c->pnew, c->cg_r, c->cg_part);
         k_ir_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal,
+                                                      c->cg_flag, graph ? 1 : 0, cond);
+    } else if (fused) {
+        k_cg_start_rows<<<nblk, kRedThreads, 0, st>>>(G, c->source, c->bcon, c->pnew, c->cg_r,
+                                                      c->cg_z, c->cg_p, c->cg_part);
+        k_cg_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal,
                                                       c->cg_flag, graph ? 1 : 0, cond);
     } else {
         k_cg_start<<<nblk, kRedThreads, 0, st>>>(G, c->source, c->pnew, c->cg_r, c->cg_z,
