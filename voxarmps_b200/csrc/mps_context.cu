@@ -552,13 +552,13 @@ int mps_init(mps_ctx* c)
     drop_graphs(c);
     TRY(vmps_neighbors(c));
     VMPS_CUDA(c, cudaMemsetAsync(c->d_max, 0, sizeof(unsigned long long), c->stream));
-    TRY(vmps_pnd(c, 0, 1, 1, c->nd));
+    TRY(vmps_pnd(c, 0, 1, 1, c->nd, true));
     TRY(device_max(c, &c->n0_s));
     if (c->cfg.re_s == c->cfg.re_l) {
         c->n0_l = c->n0_s;
     } else {
         VMPS_CUDA(c, cudaMemsetAsync(c->d_max, 0, sizeof(unsigned long long), c->stream));
-        TRY(vmps_pnd(c, 0, 1, 0, c->nds));
+        TRY(vmps_pnd(c, 0, 1, 0, c->nds, true));
         TRY(device_max(c, &c->n0_l));
     }
     VMPS_CUDA(c, cudaMemcpyAsync(c->pnew, c->p, sizeof(double) * c->n, cudaMemcpyDeviceToDevice,

@@ -462,7 +462,9 @@ int vmps_check(mps_ctx* ctx, cudaError_t e, const char* what);
 
 // stage launchers (defined in the kernel translation units)
 int vmps_neighbors(mps_ctx* ctx);
-int vmps_pnd(mps_ctx* ctx, int at_star, int correct, int which_list, double* out);
+// track_max: also the largest value into ctx->d_max (n0 at mps_init)
+int vmps_pnd(mps_ctx* ctx, int at_star, int correct, int which_list, double* out,
+             bool track_max = false);
 int vmps_max_reduce(mps_ctx* ctx, const double* a, double* result);
 int vmps_sps(mps_ctx* ctx);
 int vmps_vfraction(mps_ctx* ctx);

@@ -372,8 +372,14 @@ __global__ void __launch_bounds__(256, 8) k_lists(int n, Grid g, double cut, flo
             k += __popc(m);
         }
     }
+    // the longest row: one atomic per converged set of lanes instead of one
+    // per particle (1.6 M atomics on one address serialise in L2)
+    {
+        const unsigned act = __activemask();
+        const int km = __reduce_max_sync(act, k);
+        if ((threadIdx.x & 31) == __ffs(act) - 1) atomicMax(&len_max[which], km);
+    }
     if (q.lane == 0) {
-        atomicMax(&len_max[which], k);
         if (k > cap) {
             set_error(err, MPS_ERR_LIST_OVERFLOW);
             k = cap;
@@ -515,11 +521,15 @@ __device__ __forceinline__ void list_rows(int lane, int i0, int nq, int C, const
         scan(__shfl_sync(0xffffffffu, rb, t), __shfl_sync(0xffffffffu, rend, t));
     }
     if (lane == 0) {
+        int km = 0;
+#pragma unroll
+        for (int q = 0; q < Q; q++)
+            if (q < nq) km = max(km, k[q]);
+        atomicMax(&len_max[which], km);
 #pragma unroll
         for (int q = 0; q < Q; q++) {
             if (q >= nq) break;
             int kq = k[q];
-            atomicMax(&len_max[which], kq);
             if (kq > cap) {
                 set_error(err, MPS_ERR_LIST_OVERFLOW);
                 kq = cap;

@@ -69,6 +69,7 @@ __global__ void k_pnd(int n, Lists L, const double4* __restrict__ P4, WK wk, int
     if (q.lane == 0) {
         if (correct && wk.ktype != 2) sum = sum * ncorr;
         out[i] = sum;
+        // non-negative doubles order as their bit patterns
         if (dmax && sum > 0.0) atomicMax(dmax, (unsigned long long)__double_as_longlong(sum));
     }
 }
@@ -1056,24 +1057,27 @@ int vmps_pack(mps_ctx* c)
     return MPS_OK;
 }
 
-int vmps_pnd(mps_ctx* c, int at_star, int correct, int which, double* out)
+int vmps_pnd(mps_ctx* c, int at_star, int correct, int which, double* out, bool track_max)
 {
     double re = which == 0 ? c->cfg.re_l : c->cfg.re_s;
+    // the maximum is wanted once (n0); per step its atomics would all hit
+    // one address
+    unsigned long long* dmax = track_max ? c->d_max : nullptr;
     const double4* P = at_star ? c->P4s : c->P4;
     WK wk = make_wk(c->cfg.ktype, re);
     if (which == 0) {
         if (c->cfg.dim == 3)
             k_pnd<3, 32><<<group_blocks(c->n, 32), kBlock, 0, c->stream>>>(
-                c->n, lists(c, 0), P, wk, correct, c->cfg.ncorrection, out, c->d_max);
+                c->n, lists(c, 0), P, wk, correct, c->cfg.ncorrection, out, dmax);
         else
             k_pnd<2, 32><<<group_blocks(c->n, 32), kBlock, 0, c->stream>>>(
-                c->n, lists(c, 0), P, wk, correct, c->cfg.ncorrection, out, c->d_max);
+                c->n, lists(c, 0), P, wk, correct, c->cfg.ncorrection, out, dmax);
         vmps_count_launch(1);
     } else if (at_star && !correct && c->cfg.precision == 2 && c->P4sf) {
         // precision 2: n* from the FP32 predicted positions
         LAUNCH_SMALL(k_pnd32, c->n, lists(c, 1), c->P4sf, make_wkf(wk), out);
     } else {
-        LAUNCH_SMALL(k_pnd, c->n, lists(c, 1), P, wk, correct, c->cfg.ncorrection, out, c->d_max);
+        LAUNCH_SMALL(k_pnd, c->n, lists(c, 1), P, wk, correct, c->cfg.ncorrection, out, dmax);
     }
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
