@@ -656,6 +656,50 @@ __global__ void k_ir_start(CG A, IR I, const double* __restrict__ b, const doubl
     }
 }
 
+// The same start when the assembly has already formed r64 = b - A64 x (in
+// r64): one thread per row; rows outside the system get zeros and
+// Dirichlet rows their pressure 0 (the assembly left the guess untouched
+// for its neighbours to read).
+__global__ void __launch_bounds__(256, 8) k_ir_start_rows(CG A, IR I, const double* __restrict__ b,
+                                                          const int* __restrict__ bcon,
+                                                          double* __restrict__ x,
+                                                          double* __restrict__ r64,
+                                                          double* __restrict__ part)
+{
+    __shared__ double sh[33];
+    double bb = 0, rz = 0, rr = 0, rin = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+        float r32 = 0.f, z32 = 0.f;
+        if (A.bcon[i] == 0) {
+            const double bi = b[i], ri = r64[i];
+            r32 = (float)ri;
+            z32 = A.precond ? r32 / (float)A.diag[i] : r32;
+            bb += bi * bi;
+            rr += ri * ri;
+            rz += (double)r32 * (double)z32;
+            rin += (double)r32 * (double)r32;
+        } else {
+            r64[i] = 0.0;
+            if (bcon[i] != 0) x[i] = 0.0;
+        }
+        I.r[i] = r32;
+        I.z[i] = z32;
+        I.p[i] = z32;
+        I.d[i] = 0.f;
+        I.s[i] = 0.f;
+    }
+    bb = block_sum(bb, sh);
+    rz = block_sum(rz, sh);
+    rr = block_sum(rr, sh);
+    rin = block_sum(rin, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = bb;
+        part[A.nparts + blockIdx.x] = rz;
+        part[2 * A.nparts + blockIdx.x] = rr;
+        part[3 * A.nparts + blockIdx.x] = rin;
+    }
+}
+
 __global__ void k_ir_start_scalars(int nparts, const double* __restrict__ part, double tol2,
                                    double* scal, int* flag, int use_cond,
                                    cudaGraphConditionalHandle cond)
@@ -954,7 +998,7 @@ int vmps_ppe(mps_ctx* c)
     int warm = 0, nblk = 0;
     bool fused = false;
     {
-        int r = ppe_assemble(c, &warm, mixed ? nullptr : c->cg_r, &fused);
+        int r = ppe_assemble(c, &warm, c->cg_r, &fused);
         if (r != MPS_OK) return r;
         r = cg_grid(c, &nblk);
         if (r != MPS_OK) return r;
@@ -974,7 +1018,12 @@ int vmps_ppe(mps_ctx* c)
     cudaGraphConditionalHandle cond = 0;
     if (graph) VMPS_CUDA(c, cudaGraphConditionalHandleCreate(&cond, cgraph, 1, cudaGraphCondAssignDefault));
     IR I{c->mcv32, c->ir_d, c->ir_r, c->ir_z, c->ir_p, c->ir_s};
-    if (mixed) {
+    if (mixed && fused) {
+        k_ir_start_rows<<<nblk, kRedThreads, 0, st>>>(G, I, c->source, c->bcon, c->pnew, c->cg_r,
+                                                      c->cg_part);
+        k_ir_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal,
+                                                      c->cg_flag, graph ? 1 : 0, cond);
+    } else if (mixed) {
         k_ir_start<<<nblk, kRedThreads, 0, st>>>(G, I, c->source, c->pnew, c->cg_r, c->cg_part);
         k_ir_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal,
                                                       c->cg_flag, graph ? 1 : 0, cond);
