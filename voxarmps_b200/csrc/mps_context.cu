@@ -148,6 +148,41 @@ __global__ void k_unpermute_d(int n, const int* __restrict__ oid, const double* 
     if (i < n) out[oid[i]] = a[i];
 }
 
+// The caller-order state of mps_get_state / mps_set_state in one pass over
+// the particles: up to seven fields between cell order and the staging
+// area (field k at stage + k * pitch), so that the host copies run back to
+// back with one synchronisation.
+struct StateIO {
+    double* f[7];  // cell-order fields (null: not transferred)
+    double* pnew;  // set: also receives p
+};
+
+__global__ void k_state_out(int n, long pitch, const int* __restrict__ oid, StateIO s,
+                            double* __restrict__ stage)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int o = oid[i];
+#pragma unroll
+    for (int k = 0; k < 7; k++)
+        if (s.f[k]) stage[k * pitch + o] = s.f[k][i];
+}
+
+__global__ void k_state_in(int n, long pitch, const int* __restrict__ oid, StateIO s,
+                           const double* __restrict__ stage)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int o = oid[i];
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+        if (!s.f[k]) continue;
+        const double v = stage[k * pitch + o];
+        s.f[k][i] = v;
+        if (k == 6 && s.pnew) s.pnew[i] = v;
+    }
+}
+
 __global__ void k_unpermute_i(int n, const int* __restrict__ oid, const int* __restrict__ a,
                               int* __restrict__ out)
 {
@@ -270,6 +305,7 @@ int allocate(mps_ctx* c)
     TRY(dalloc(c, &c->bx_s, P));
     TRY(dalloc(c, &c->key_s, P));
     TRY(dalloc(c, &c->stage_in, P));
+    TRY(dalloc(c, &c->stage_io, 7 * (size_t)P));
     TRY(dalloc(c, &c->P4, P));
     TRY(dalloc(c, &c->P4s, P));
     TRY(dalloc(c, &c->P4c, P));
@@ -843,16 +879,19 @@ int mps_set_state(mps_ctx* c, const double* x, const double* y, const double* z,
     NEED_INIT(c);
     VMPS_CUDA(c, cudaSetDevice(c->device));
     const int n = c->n;
+    const long P = c->pitch;
     const double* src[7] = {x, y, z, u, v, w, p};
     double* dst[7] = {c->x, c->y, c->z, c->u, c->v, c->w, c->p};
+    StateIO io{};
     for (int k = 0; k < 7; k++) {
         if (!src[k] || (c->cfg.dim == 2 && (k == 2 || k == 5))) continue;
-        VMPS_CUDA(c, cudaMemcpyAsync(c->stage_in, src[k], sizeof(double) * n,
+        VMPS_CUDA(c, cudaMemcpyAsync(c->stage_io + k * P, src[k], sizeof(double) * n,
                                      cudaMemcpyHostToDevice, c->stream));
-        k_permute_in<<<grid_blocks(n), kBlock, 0, c->stream>>>(n, c->oid, c->stage_in, dst[k],
-                                                               k == 6 ? c->pnew : nullptr);
-        vmps_count_launch(1);
+        io.f[k] = dst[k];
     }
+    io.pnew = c->pnew;
+    k_state_in<<<grid_blocks(n), kBlock, 0, c->stream>>>(n, P, c->oid, io, c->stage_io);
+    vmps_count_launch(1);
     TRY(vmps_pack(c));
     VMPS_CUDA(c, cudaGetLastError());
     return MPS_OK;
@@ -961,12 +1000,21 @@ int mps_get_state(mps_ctx* c, double* x, double* y, double* z, double* u, double
                   double* p)
 {
     NEED_INIT(c);
-    const char* names[7] = {"x", "y", "z", "u", "v", "w", "p"};
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    const int n = c->n;
+    const long P = c->pitch;
     double* out[7] = {x, y, z, u, v, w, p};
-    for (int k = 0; k < 7; k++) {
-        if (!out[k] || (c->cfg.dim == 2 && (k == 2 || k == 5))) continue;
-        TRY(mps_download(c, names[k], out[k], nullptr));
-    }
+    double* from[7] = {c->x, c->y, c->z, c->u, c->v, c->w, c->p};
+    StateIO io{};
+    for (int k = 0; k < 7; k++)
+        if (out[k] && !(c->cfg.dim == 2 && (k == 2 || k == 5))) io.f[k] = from[k];
+    k_state_out<<<grid_blocks(n), kBlock, 0, c->stream>>>(n, P, c->oid, io, c->stage_io);
+    vmps_count_launch(1);
+    for (int k = 0; k < 7; k++)
+        if (io.f[k])
+            VMPS_CUDA(c, cudaMemcpyAsync(out[k], c->stage_io + k * P, sizeof(double) * n,
+                                         cudaMemcpyDeviceToHost, c->stream));
+    VMPS_CUDA(c, cudaStreamSynchronize(c->stream));
     return MPS_OK;
 }
 

@@ -237,7 +237,8 @@ struct mps_ctx {
     int* len_max = nullptr;         // [0] max len_l, [1] max len_s (diagnostics)
     unsigned long long* d_max = nullptr;  // atomic max of a non-negative double
     int* scan_tmp = nullptr;        // tile sums of the cell-count scans
-    double* stage_in = nullptr;     // H2D staging for mps_set_state
+    double* stage_in = nullptr;     // H2D staging for mps_set_field / mps_set_rows
+    double* stage_io = nullptr;     // 7 x pitch: mps_set_state / mps_get_state staging
     // profiling (CUDA events on the context stream)
     bool profile = false;
     cudaEvent_t ev[8] = {};
