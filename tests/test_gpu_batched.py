@@ -12,14 +12,16 @@ from gpu_util import gpu_cfg, rel_err
 pytestmark = pytest.mark.gpu
 
 
-def test_four_scenes_match_separate_runs():
+@pytest.mark.parametrize("precision", [0, 1])
+def test_four_scenes_match_separate_runs(precision):
+    """In FP64 and in mixed precision (each scene's CG to its own residual)."""
     l0 = 0.01
     scenes = [cases.dam_break(2, l0, (w, h), (100, 60)) for w, h in ((10, 20), (25, 50), (18, 33),
                                                                      (40, 25))]
     base = config.reference_defaults(l0, 2)
     base.update(re_s=2.1 * l0, re_l=4.0 * l0, dt=1e-4, gy=-9.81)
     base = gpu_cfg(base, cg_tol=1e-12)
-    cfg, case, sid, boxes, pmax = config.batched(base, scenes)
+    cfg, case, sid, boxes, pmax = config.batched(dict(base, precision=precision), scenes)
     g = vm.Solver(cfg, case)
     g.set_scenes(sid, boxes, pmax)
     assert g.init() == 0
