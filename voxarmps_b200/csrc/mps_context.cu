@@ -1208,8 +1208,9 @@ void* mps_stream(mps_ctx* c) { return c ? (void*)c->stream : nullptr; }
 //     x y z u v w p pnew phat un vn wn rho n pold
 //   int32 ptype[n], scene[n]; then, when nscenes > 1, double boxes[6 ns],
 //   pmax[ns];  uint64 FNV-1a hash of every preceding byte.
-// Resuming replays the counting sort by (cell, id) at the next step, so a
-// resumed run continues bit for bit.
+// Resuming replays the counting sort by (cell, x, id) at the next step,
+// which does not depend on the slot order before it, so a resumed run
+// continues bit for bit.
 
 static const char kCkMagic[8] = {'V', 'X', 'M', 'P', 'S', 'C', 'K', '1'};
 static const char* kCkFields[15] = {"x",  "y",  "z",  "u",   "v", "w", "p", "pnew",

@@ -8,11 +8,11 @@
 //                  bucket counts by atomics;
 //   2. scan        exclusive prefix sums of the counts (cell starts);
 //   3. k_scatter   particles into their cell bucket (arbitrary order);
-//   4. k_rank      order inside a bucket: by (x, original id) on the
-//                  Laplacian grid, so that every x-triple of cells is sorted
-//                  by x; by original id on the PND grid, the stable counting
-//                  sort of the reference's insertion loop (functions.cu:2820);
-//                  NEIGHBOR's own Laplacian-grid order is formed on download;
+//   4. k_rank      order inside a bucket by (x, original id) on both grids,
+//                  so that every x-triple of cells is sorted by x; NEIGHBOR's
+//                  own order, (cell, id) -- the stable counting sort of the
+//                  reference's insertion loop (functions.cu:2820) -- is
+//                  formed when a permutation is downloaded;
 //   5. k_gather    reorder the persistent particle state into cell order;
 //   6. k_lists     both lists, membership decided with the reference's exact
 //                  FP64 arithmetic; Q particles of one cell per warp for the
