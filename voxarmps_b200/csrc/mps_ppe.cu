@@ -34,6 +34,9 @@ constexpr int kRedThreads = 256;
 // assembly runs 16 lanes per row (PPE stage 12.4 ms against 12.8 ms at 32)
 constexpr int kRowG = 32;
 constexpr int kAsmG = 16;
+// lanes per row of the mixed-precision products (inner FP32 and refinement):
+// 16 (config 2 at 19.37 ms/step against 19.63 ms with 32 or 8 lanes)
+constexpr int kIrG = 16;
 
 __device__ __forceinline__ double block_sum(double v, double* sh)
 {
@@ -254,17 +257,17 @@ struct CG {
 // per product and loaded evict-first (ld.global.cs), which keeps the
 // gathered vector in L1/L2: 0.61 against 0.755 ms per launch after 700 steps
 // of the 1.6 M-particle dam, equal on its first steps.
-template <typename V>
-__device__ __forceinline__ double spmv_row(const CG& A, const Grp<kRowG>& q,
+template <typename V, int G = kRowG>
+__device__ __forceinline__ double spmv_row(const CG& A, const Grp<G>& q,
                                            const V* __restrict__ v, int i, int off, int L)
 {
     const int* __restrict__ c = A.mcol + off;
     const double* __restrict__ a = A.mval + off;
     double acc0 = 0.0, acc1 = 0.0;
     int k = q.lane;
-    for (; k + kRowG < L; k += 2 * kRowG) {
-        int c0 = __ldcs(c + k), c1 = __ldcs(c + k + kRowG);
-        double a0 = __ldcs(a + k), a1 = __ldcs(a + k + kRowG);
+    for (; k + G < L; k += 2 * G) {
+        int c0 = __ldcs(c + k), c1 = __ldcs(c + k + G);
+        double a0 = __ldcs(a + k), a1 = __ldcs(a + k + G);
         acc0 += a0 * (double)v[c0];
         acc1 += a1 * (double)v[c1];
     }
@@ -284,23 +287,24 @@ __device__ __forceinline__ double spmv_row_warp(const CG& A, const Grp<kRowG>& q
 // FP32 products and accumulation, same warp-per-row layout.  The FP32 copy
 // interleaves each entry's column and value bits (one 8-byte load per
 // entry), and each lane keeps four entries in flight.
+template <int G = kRowG>
 __device__ __forceinline__ float spmv_row_warp32(const CG& A, const int2* __restrict__ cv,
-                                                 const Grp<kRowG>& q, const float* __restrict__ v,
+                                                 const Grp<G>& q, const float* __restrict__ v,
                                                  int i, int off, int L)
 {
     const int2* __restrict__ e = cv + off;
     float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc3 = 0.f;
     int k = q.lane;
-    for (; k + 3 * kRowG < L; k += 4 * kRowG) {
-        const int2 e0 = __ldcs(e + k), e1 = __ldcs(e + k + kRowG), e2 = __ldcs(e + k + 2 * kRowG),
-                   e3 = __ldcs(e + k + 3 * kRowG);
+    for (; k + 3 * G < L; k += 4 * G) {
+        const int2 e0 = __ldcs(e + k), e1 = __ldcs(e + k + G), e2 = __ldcs(e + k + 2 * G),
+                   e3 = __ldcs(e + k + 3 * G);
         acc0 = __fmaf_rn(__int_as_float(e0.y), v[e0.x], acc0);
         acc1 = __fmaf_rn(__int_as_float(e1.y), v[e1.x], acc1);
         acc2 = __fmaf_rn(__int_as_float(e2.y), v[e2.x], acc2);
         acc3 = __fmaf_rn(__int_as_float(e3.y), v[e3.x], acc3);
     }
-    for (; k + kRowG < L; k += 2 * kRowG) {
-        const int2 e0 = __ldcs(e + k), e1 = __ldcs(e + k + kRowG);
+    for (; k + G < L; k += 2 * G) {
+        const int2 e0 = __ldcs(e + k), e1 = __ldcs(e + k + G);
         acc0 = __fmaf_rn(__int_as_float(e0.y), v[e0.x], acc0);
         acc1 = __fmaf_rn(__int_as_float(e1.y), v[e1.x], acc1);
     }
@@ -734,8 +738,8 @@ __global__ void k_ir_spmv(CG A, IR I, double* __restrict__ r64, double* __restri
     __shared__ double sh[33];
     if (flag[0]) return;
     const int phase = flag[2];
-    Grp<kRowG> q;
-    const long nwarps = (long)gridDim.x * blockDim.x / kRowG;
+    Grp<kIrG> q;
+    const long nwarps = (long)gridDim.x * blockDim.x / kIrG;
     double acc = 0;
     for (long w = q.gid; w < A.n; w += nwarps) {
         int i = (int)w;
