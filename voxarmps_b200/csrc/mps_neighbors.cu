@@ -264,12 +264,11 @@ __global__ void k_translate(int n, const int* __restrict__ inv, const int* __res
 // of x.  Rows are stored in scan order (y, z outer, memory order inside);
 // the reference's own order (x offset outermost, ascending id per cell) is
 // restored when lists are exported (mps_download_lists).
-// 8 resident blocks per SM (32 registers, a few bytes of spills in 3D):
-// the PND-radius list stage 0.16 ms faster than at 48 registers on the
-// 1.6 M-particle dam (6 blocks: 0.08 ms; the Laplacian list's k_lists_q
-// loses at 5 blocks, its spills grow)
+// 6 resident blocks per SM (40 registers): with the warp's groups stepping
+// together, the neighbour stage 4.51 ms on the 1.6 M-particle dam against
+// 4.61 ms at 8 blocks (32 registers, spills) and 4.69 ms for divergent groups
 template <int DIM, int G>
-__global__ void __launch_bounds__(256, 8) k_lists(int n, Grid g, double cut, float cut_lo, float cut_hi, int cap,
+__global__ void __launch_bounds__(256, 6) k_lists(int n, Grid g, double cut, float cut_lo, float cut_hi, int cap,
                         const double4* __restrict__ P4, const float4* __restrict__ P4f,
                         const int* __restrict__ cell, const int* __restrict__ cst,
                         const int* __restrict__ cnt, const int* __restrict__ perm,
@@ -277,9 +276,13 @@ __global__ void __launch_bounds__(256, 8) k_lists(int n, Grid g, double cut, flo
                         int* __restrict__ out, int* __restrict__ len, int* len_max, int which,
                         unsigned int* err)
 {
+    // The warp's 32 / G groups step through their runs together (every
+    // loop trip count is the warp's largest, lanes past their own run's end
+    // idle): divergent groups would replay each ballot and shuffle once per
+    // group.  Groups past the last row take part with empty runs.
     Grp<G> q;
-    int i = (int)q.gid;
-    if (i >= n) return;  // whole groups leave together (n rows, G lanes each)
+    const bool live = q.gid < n;
+    const int i = live ? (int)q.gid : 0;
     double4 pi = P4[i];
     float4 fi = P4f[i];
     int C = cell[i] - 1;
@@ -303,9 +306,10 @@ __global__ void __launch_bounds__(256, 8) k_lists(int n, Grid g, double cut, flo
         return d > 0 ? d * d : 0.0;
     };
     const double gxl = gap2(-1, lox, hix), gxh = gap2(1, lox, hix);
-    const int ndp = m6 - m5 + 1, nt = (m4 - m3 + 1) * ndp;
+    const int ndp = m6 - m5 + 1, nt = live ? (m4 - m3 + 1) * ndp : 0;
     // the windows of this lane's runs t = lane, lane + G, ...
-    constexpr int R = ((DIM == 3 ? 9 : 3) + G - 1) / G;
+    constexpr int NT = DIM == 3 ? 9 : 3;
+    constexpr int R = (NT + G - 1) / G;
     int wb[R], we[R];
 #pragma unroll
     for (int u = 0; u < R; u++) {
@@ -337,49 +341,48 @@ __global__ void __launch_bounds__(256, 8) k_lists(int n, Grid g, double cut, flo
     }
     int* row = out + (size_t)i * cap;
     int k = 0;
+    const unsigned full = 0xffffffffu;
 #pragma unroll
-    for (int t = 0; t < (DIM == 3 ? 9 : 3); t++) {
-        if (t >= nt) break;
+    for (int t = 0; t < NT; t++) {
         const int src_lane = (int)q.base + t % G;
-        const int b = __shfl_sync(q.mask, wb[t / G], src_lane);
-        const int e = __shfl_sync(q.mask, we[t / G], src_lane);
-        for (int base = b; base < e; base += G) {
-            int jj = base + q.lane;
+        const int b = __shfl_sync(full, wb[t / G], src_lane);
+        const int e = __shfl_sync(full, we[t / G], src_lane);
+        const int trips = __reduce_max_sync(full, (e - b + G - 1) / G);
+        for (int it = 0; it < trips; it++) {
+            const int jj = b + it * G + q.lane;
+            const bool valid = jj < e;
             bool in = false;
             int j = 0;
-            if (jj < e) {
+            if (valid) {
                 j = perm[jj];
                 // FP32 screen; the exact FP64 rule decides only inside
                 // the screening margin [cut_lo, cut_hi]
-                float4 fj = P4f[j];
-                float ex = fj.x - fi.x, ey = fj.y - fi.y, ez = DIM == 3 ? fj.z - fi.z : 0.f;
+                const float4 fj = P4f[j];
+                const float ex = fj.x - fi.x, ey = fj.y - fi.y,
+                            ez = DIM == 3 ? fj.z - fi.z : 0.f;
                 // fused multiply-adds: fewer roundings than the bound assumes
-                float f2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
+                const float f2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
                 if (f2 < cut_lo) {
                     in = (DIM == 3) || (j != i);
                 } else if (f2 <= cut_hi) {
-                    double4 pj = P4[j];
-                    double d2 = dist2<DIM>(pj.x - pi.x, pj.y - pi.y,
-                                           DIM == 3 ? pj.z - pi.z : 0.0);
+                    const double4 pj = P4[j];
+                    const double d2 = dist2<DIM>(pj.x - pi.x, pj.y - pi.y,
+                                                 DIM == 3 ? pj.z - pi.z : 0.0);
                     in = (DIM == 3) ? (d2 <= cut) : (j != i && d2 < cut);
                 }
             }
-            unsigned m = q.ballot(in);
+            const unsigned m = (__ballot_sync(full, in) >> q.base) & ((1u << G) - 1u);
             if (in) {
-                int pos = k + __popc(m & ((1u << q.lane) - 1u));
+                const int pos = k + __popc(m & ((1u << q.lane) - 1u));
                 if (pos < cap) row[pos] = j;
             }
             k += __popc(m);
         }
     }
-    // the longest row: one atomic per converged set of lanes instead of one
-    // per particle (1.6 M atomics on one address serialise in L2)
-    {
-        const unsigned act = __activemask();
-        const int km = __reduce_max_sync(act, k);
-        if ((threadIdx.x & 31) == __ffs(act) - 1) atomicMax(&len_max[which], km);
-    }
-    if (q.lane == 0) {
+    // the longest row: one atomic per warp instead of one per particle
+    const int km = __reduce_max_sync(full, live ? k : 0);
+    if ((threadIdx.x & 31) == 0) atomicMax(&len_max[which], km);
+    if (live && q.lane == 0) {
         if (k > cap) {
             set_error(err, MPS_ERR_LIST_OVERFLOW);
             k = cap;
