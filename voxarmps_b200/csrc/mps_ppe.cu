@@ -89,14 +89,20 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
                            int2* __restrict__ mrow, const int* __restrict__ own,
                            int* __restrict__ sysmask, double* __restrict__ r0)
 {
+    // The warp's two row groups step through their rows together (the trip
+    // count is the warp's largest; lanes past their row's end idle), so the
+    // ballot is one warp instruction rather than one per diverged group;
+    // groups past the last row, and rows outside the system, take part with
+    // no entries.
     Grp<kAsmG> q;
-    int i = (int)q.gid;
-    if (i >= n) return;
-    int bi = bcon[i];
+    const bool live = q.gid < n;
+    const int i = live ? (int)q.gid : 0;
+    const int bi = bcon[i];
     const bool mine = own[i] != 0;
-    if (q.lane == 0) sysmask[i] = (bi != 0 || !mine) ? 1 : 0;
-    if (bi != 0) {
-        if (q.lane == 0) {
+    const bool work = live && bi == 0 && mine;
+    if (live && q.lane == 0) {
+        sysmask[i] = (bi != 0 || !mine) ? 1 : 0;
+        if (bi != 0) {
             mlen[i] = 0;
             mrow[i] = make_int2(moff[i], -1);
             diag[i] = 0.0;
@@ -105,26 +111,23 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
             // with r0 the rows read every neighbour's guess: CG's start
             // zeroes this one instead
             if (!r0) pnew[i] = 0.0;
-        }
-        return;
-    }
-    if (!mine) {  // a ghost: its row belongs to its owner's system, its value arrives
-        if (q.lane == 0) {  // from the owner (a column here, not a row)
-            mlen[i] = 0;
+        } else if (!mine) {  // a ghost: its row belongs to its owner's system, its
+            mlen[i] = 0;     // value arrives from the owner (a column here, not a row)
             mrow[i] = make_int2(moff[i], -1);
             diag[i] = 0.0;
             source[i] = 0.0;
         }
-        return;
     }
-    double4 pi = P4[i];
+    const double4 pi = P4[i];
     const int* row = nbr + (size_t)i * cap;
     int* crow = mcol + moff[i];
     double* vrow = mval + moff[i];
     double dg = 0.0, ax = 0.0;
-    int cnt = 0, L = len[i];
-    for (int base = 0; base < L; base += kAsmG) {
-        int k = base + q.lane;
+    int cnt = 0;
+    const int L = work ? len[i] : 0;
+    const int trips = __reduce_max_sync(0xffffffffu, (L + kAsmG - 1) / kAsmG);
+    for (int it = 0; it < trips; it++) {
+        int k = it * kAsmG + q.lane;
         double v = 0.0, xj = 0.0;
         int j = -1;
         bool keep = false;
@@ -150,7 +153,7 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
             }
         }
         dg += v;
-        unsigned m = q.ballot(keep);
+        const unsigned m = (__ballot_sync(0xffffffffu, keep) >> q.base) & ((1u << kAsmG) - 1u);
         if (keep) {
             int pos = cnt + __popc(m & ((1u << q.lane) - 1u));
             crow[pos] = j;
@@ -162,7 +165,7 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
     }
     dg = q.sum(dg);
     if (r0) ax = q.sum(ax);
-    if (q.lane == 0) {
+    if (work && q.lane == 0) {
         diag[i] = dg + A.reg;
         mlen[i] = cnt;
         mrow[i] = make_int2(moff[i], cnt);
