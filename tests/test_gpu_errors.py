@@ -53,3 +53,31 @@ def test_stage_calls_before_init_rejected():
     g = vm.Solver(gpu_cfg(cfg), case)
     with pytest.raises(vm.MpsError):
         g.step()
+
+
+@pytest.mark.parametrize("which", ["dam2d", "dam3d"])
+def test_nonfinite_position_keeps_the_sort_a_permutation(which):
+    """A particle whose position is NaN (and one at infinity) lands in cell 1
+    with MPS_ERR_CELL; the in-cell order by (x, id) still gives every slot
+    exactly once (x's order key places NaN and infinities at the ends), so
+    the permutations stay permutations and further steps run and report."""
+    cfg, case = config.baseline(0) if which == "dam2d" else config.scaled_dam3d(1)
+    case = dict(case)
+    case["x"] = case["x"].copy()
+    fluid = np.flatnonzero(np.asarray(case["ptype"]) > 0)
+    case["x"][fluid[-1]] = np.nan
+    case["x"][fluid[-2]] = np.inf
+    g = vm.Solver(gpu_cfg(cfg), case)
+    r = g.init()
+    assert r & vm.MPS_ERR_CELL
+    n = len(case["x"])
+    for sfx in ("l", "s"):
+        perm = g.get("perm_" + sfx)
+        assert np.array_equal(np.sort(perm), np.arange(n)), sfx
+    for _ in range(2):
+        r = g.step()
+        assert r & (vm.MPS_ERR_CELL | vm.MPS_ERR_NAN | vm.MPS_ERR_BOX)
+    for sfx in ("l", "s"):
+        perm = g.get("perm_" + sfx)
+        assert np.array_equal(np.sort(perm), np.arange(n)), sfx
+    g.close()
