@@ -44,3 +44,31 @@ def test_four_scenes_match_separate_runs(precision):
             if f == "y":
                 part = part - (case["y"][sid == k].min() - scenes[k]["y"].min())
             assert rel_err(part, ref) <= 1e-7, (f, k)
+
+
+def test_config4_batch_matches_separate_runs():
+    """The batched configuration itself: 64 scenes of 800 to 9,600 fluid
+    particles in one context, mixed-precision PPE, two steps, against one
+    FP64 oracle run per scene.  Both solve each scene's PPE to 1e-8; the
+    bounds are the mixed mode's measured error against FP64 with margin."""
+    base, scenes = config.baseline(4)
+    base = gpu_cfg(base, cg_tol=1e-8, precision=1)
+    cfg, case, sid, boxes, pmax = config.batched(base, scenes)
+    g = vm.Solver(cfg, case)
+    g.set_scenes(sid, boxes, pmax)
+    assert g.init() == 0
+    for _ in range(2):
+        assert g.step() == 0
+    assert g.scalar("cg_relres") <= 1e-8
+    tol = {"x": 1e-9, "y": 1e-9, "u": 1e-5, "v": 1e-5, "p": 1e-5}
+    got = {f: g.get(f) for f in tol}
+    for k, sc in enumerate(scenes):
+        o = pyoracle.Oracle(config.with_box(dict(base, precision=0), sc), sc)
+        assert o.init() == 0
+        for _ in range(2):
+            o.step()
+        for f, t in tol.items():
+            part = got[f][sid == k]
+            if f == "y":
+                part = part - (case["y"][sid == k].min() - sc["y"].min())
+            assert rel_err(part, o.get(f)) <= t, (f, k)

@@ -10,7 +10,8 @@ each at the initial lattice and again after 20 GPU steps, when particles
 have left the lattice: the lists are rebuilt at the GPU's own positions
 (mps_neighbors) and the oracle bins the same positions.  Along long runs
 too: the 2D dam over its whole 2000 steps and a small 3D dam over 600, at
-the splashing states the collapse produces.
+the splashing states the collapse produces.  And one whole step of the
+headline dam against the oracle's.
 """
 import numpy as np
 import pytest
@@ -18,7 +19,7 @@ import pytest
 import pyoracle
 import voxarmps_b200 as vm
 from voxarmps_b200 import config
-from gpu_util import gpu_cfg
+from gpu_util import gpu_cfg, pair, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -91,3 +92,21 @@ def test_dam2d_whole_run_lists_bit_exact():
 def test_dam3d_small_long_run_lists_bit_exact():
     cfg, case = config.scaled_dam3d(1)
     run_long(gpu_cfg(cfg), case, 600, 100)
+
+
+def test_dam3d_headline_one_step_matches_oracle():
+    """One step of the 1,595,308-particle dam on the CUDA path and on the
+    oracle: the FP64 stage outputs within a few ulps, the pressures (two
+    FP64 CG runs to 1e-12, different dot orders) within 1e-7."""
+    cfg, case = config.baseline(1)
+    cfg = gpu_cfg(cfg, cg_tol=1e-12)
+    g, o = pair(cfg, case)
+    assert g.step() == 0
+    assert o.step() == 0
+    for f in ("xs", "ys", "zs", "us", "vs", "ws", "nstar"):
+        assert rel_err(g.get(f), o.get(f)) <= 1e-12, f
+    assert np.array_equal(g.get("bcon"), o.get("bcon"))
+    assert rel_err(g.get("source"), o.get("source")) <= 1e-12
+    for f in ("x", "y", "z", "u", "v", "w", "p"):
+        assert rel_err(g.get(f), o.get(f)) <= 1e-7, f
+    g.close()

@@ -28,6 +28,9 @@ def small_3d():
 CASES = {
     "config0": lambda: config.baseline(0),
     "dam3d_small": small_3d,
+    # the two-phase configuration at its full geometry (86,118 particles;
+    # SPS-LES, Herschel-Bulkley second fluid)
+    "config3": lambda: config.baseline(3),
 }
 
 
