@@ -141,3 +141,24 @@ def test_fp32_pnd_and_gradient_against_fp64(which):
         assert errs[f] <= FP32_EXPLICIT_U, f
     for f in ("x", "y", "z"):
         assert errs[f] <= FP32_EXPLICIT_X, f
+
+
+def test_full_size_mixed_error_at_benchmark_tolerance():
+    """The 1.6 M-particle dam at the benchmark's own tolerance (1e-8): the
+    mixed-precision run against the FP64 run after 10 steps, the figures
+    bench.py --config 2 reports as error_vs_fp64 (measured: pressure 4.8e-7
+    of its maximum, positions 1.1e-13, velocities 1.9e-7); the bounds leave
+    a factor 10."""
+    cfg, case = config.baseline(1)
+    out = {}
+    for prec in (0, 1):
+        g = vm.Solver(gpu_cfg(cfg, precision=prec, cg_tol=1e-8), case)
+        assert g.init() == 0
+        g.set_graph(True)
+        for _ in range(10):
+            assert g.step() == 0
+        out[prec] = {f: g.get(f) for f in ("x", "y", "z", "u", "v", "w", "p")}
+        g.close()
+    bounds = {"p": 5e-6, "x": 1e-12, "y": 1e-12, "z": 1e-12, "u": 2e-6, "v": 2e-6, "w": 2e-6}
+    for f, b in bounds.items():
+        assert rel_err(out[1][f], out[0][f]) <= b, f
