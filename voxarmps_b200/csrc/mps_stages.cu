@@ -305,6 +305,11 @@ __global__ void k_sps2(int n, Lists L, Phys P, const int* __restrict__ ptype,
 struct PredArgs {
     WK ws, wl;
     double n0_s, visc_coef, dt, gx, gy, gz, relaxp, rho1, rho2;
+    // Newtonian fluids: VISCOSITY sets meu by particle kind (nu1 rho1 for
+    // kinds <= 1, nu2 rho2 for kind 2), so a neighbour's meu follows from the
+    // kind its packed position carries, without a gather of meu
+    int meu_by_kind;
+    double meu1, meu2;
 };
 
 // PREDICTION (functions.cu:2283-2369), first part: the explicit pressure
@@ -406,7 +411,7 @@ k_predict32(int n, Lists Ll, PredArgs A, WKf wl, const double* __restrict__ meu,
         const float W = w_fast32<DIM>(wl, d2);
         float NEU = neu_same;
         if ((int)fj.w != pI) {
-            const double mJ = meu[J];
+            const double mJ = A.meu_by_kind ? ((int)fj.w == 2 ? A.meu2 : A.meu1) : meu[J];
             NEU = (float)(2 * mI * mJ / (mI + mJ) / rhoI);
         }
         const float du = W * (vj.x - vi.x), dv = W * (vj.y - vi.y);
@@ -504,7 +509,7 @@ k_predict(int n, Lists Ll, PredArgs A, const double* __restrict__ meu,
         double W = w_fast<DIM>(A.wl, d2, rsq(d2));
         double NEU = neu_same;
         if ((int)pj.w != pI) {
-            double mJ = meu[J];
+            const double mJ = A.meu_by_kind ? ((int)pj.w == 2 ? A.meu2 : A.meu1) : meu[J];
             NEU = 2 * mI * mJ / (mI + mJ) / rhoI;
         }
         double4 uj = U4[J];
@@ -1137,6 +1142,10 @@ int vmps_predict(mps_ctx* c)
     A.visc_coef = 4 * f.dt / (c->lambda_l * c->n0_l);
     A.dt = f.dt; A.gx = f.gx; A.gy = f.gy; A.gz = f.gz; A.relaxp = f.relaxp;
     A.rho1 = f.rho1; A.rho2 = f.rho2;
+    // the same products VISCOSITY forms (k_viscosity, fluid2_type 0)
+    A.meu_by_kind = f.fluid2_type == 0 ? 1 : 0;
+    A.meu1 = f.nu1 * f.rho1;
+    A.meu2 = f.nu2 * f.rho2;
     LAUNCH_SMALL(k_predict_p, c->n, lists(c, 1), A, c->P4, c->pnew, c->phat, c->rho, c->pres_x,
                  c->pres_y, c->pres_z);
     // without SPS, neut is 0 and the eddy-viscosity sums are left out
