@@ -310,6 +310,7 @@ int allocate(mps_ctx* c)
     TRY(dalloc(c, &c->P4s, P));
     TRY(dalloc(c, &c->P4c, P));
     TRY(dalloc(c, &c->U4, P));
+    TRY(dalloc(c, &c->PP4, P));
     TRY(dalloc(c, &c->P4f, P));
     if (c->cfg.precision >= 1) TRY(dalloc(c, &c->U4f, P));
     if (c->cfg.precision == 2) {

@@ -195,6 +195,7 @@ struct mps_ctx {
     // packed gathers: positions (x, y, z, ptype), predicted positions,
     // collision output, velocities (u, v, w, -) and (pnew, phat) pairs
     double4 *P4 = nullptr, *P4s = nullptr, *P4c = nullptr, *U4 = nullptr;
+    double4* PP4 = nullptr;  // (x, y, z, previous pressure) for PREDICTION's pressure sums
     float4* P4f = nullptr;   // positions relative to the box minimum, FP32, w = ptype
     float4* U4f = nullptr;   // velocities, FP32 (mixed precision's viscous sums)
     float4* P4sf = nullptr;  // precision 2: predicted positions relative to the box, FP32
