@@ -73,6 +73,32 @@ struct Asm {
     int matopt, srcopt;
 };
 
+// The w slot of the predicted positions for an assembly that forms CG's
+// starting residual: the guess (pnew) of an unknown (bcon 0), a NaN whose
+// low bits code the status otherwise (1: Dirichlet, 2: outside, bcon -1).
+// A pressure that has gone NaN reads as an unknown with a NaN guess, as a
+// separate gather of it would.
+__device__ __forceinline__ double wguess_code(int b)
+{
+    return __longlong_as_double((long long)(0x7FF8000000000000ull | (b == 1 ? 1ull : 2ull)));
+}
+
+__device__ __forceinline__ int wguess_status(double w)
+{
+    if (w == w) return 0;
+    const unsigned long long code = (unsigned long long)__double_as_longlong(w) & 3ull;
+    return code == 1 ? 1 : (code == 2 ? -1 : 0);
+}
+
+__global__ void k_pack_wguess(int n, const int* __restrict__ bcon, const double* __restrict__ pnew,
+                              double4* __restrict__ P4s)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int b = bcon[i];
+    reinterpret_cast<double*>(P4s + i)[3] = b == 0 ? pnew[i] : wguess_code(b);
+}
+
 // one lane group (kAsmG lanes) per row; the non-zero columns are compacted in list order into
 // the row's CSR segment (capacity = the row's list length)
 template <int DIM>
@@ -133,13 +159,19 @@ __global__ void __launch_bounds__(256, 6) k_assemble(int n, int cap, Asm A, cons
         bool keep = false;
         if (k < L) {
             j = row[k];
-            if (r0) xj = pnew[j];  // the initial guess, read beside the position
             double4 pj;
             int bj;
-            if (w_bcon) {  // P4's w slot holds bcon: one gather
+            if (w_bcon == 2) {  // w: the guess of an unknown, a coded NaN otherwise
+                pj = P4[j];
+                xj = pj.w;
+                bj = wguess_status(pj.w);
+                if (j == i) bj = -1;
+            } else if (w_bcon) {  // P4's w slot holds bcon: one gather
+                if (r0) xj = pnew[j];  // the initial guess, read beside the position
                 pj = P4[j];
                 bj = j == i ? -1 : (int)pj.w;
             } else {
+                if (r0) xj = pnew[j];
                 bj = j == i ? -1 : bcon[j];
                 if (bj != -1) pj = P4[j];
             }
@@ -948,7 +980,16 @@ static int ppe_assemble(mps_ctx* c, int* warm_out, double* r0 = nullptr, bool* f
     // the predicted positions carry bcon in their w slot when BCON ran after
     // the last PREDICTION (always within a step; the per-stage entry points
     // may be called out of order)
-    const int w_bcon = (f.ppe_at_predicted && c->p4s_bcon) ? 1 : 0;
+    int w_bcon = (f.ppe_at_predicted && c->p4s_bcon) ? 1 : 0;
+    if (r0 && f.ppe_at_predicted) {
+        // with the residual formed here every kept column also needs its
+        // guess: the w slot carries it for the unknowns and a coded NaN for
+        // the other kinds, so one gather brings position, status and guess
+        k_pack_wguess<<<grid_blocks(n), kBlock, 0, st>>>(n, c->bcon, c->pnew, c->P4s);
+        vmps_count_launch(1);
+        w_bcon = 2;
+        c->p4s_bcon = false;  // the w slot no longer holds bcon alone
+    }
     if (f.dim == 3)
         k_assemble<3><<<wblocks, kBlock, 0, st>>>(n, c->cap_l, A, c->nbr_l, c->len_l, c->bcon, P4,
                                                   nsrc, warm, c->pnew, c->pold, c->moff, c->mcol,
