@@ -8,7 +8,8 @@ A step is one full MPS time step (neighbour search, PND, prediction, PPE
 assembly + CG to the stated relative residual, gradient, integration,
 collision, commit).  ``value`` is whole-job particle-steps/s with the state
 resident in HBM; ``e2e`` is the same metric through the public API with host
-buffers (state uploaded from pinned host memory and downloaded every step).
+buffers (state uploaded from pinned host memory and downloaded every step,
+through ``mps_step_io``).
 Under torchrun each rank advances its own copy of the scene (independent
 scenes, no collective on the data path: weak scaling), except that the
 batched configuration (--config 4) splits its 64 scenes between the ranks
@@ -440,9 +441,9 @@ def run_ours(args):
     e3 = torch.cuda.Event(enable_timing=True)
     e2.record(stream)
     for _ in range(args.steps):
-        s.set_state(*ptrs)
-        s.step()
-        s.get_state(*ptrs)
+        # mps_step_io: mps_set_state + mps_step + mps_get_state in one call,
+        # the copy of u, v, w, p overlapped with the neighbour search
+        s.step_io(ptrs, ptrs)
     e3.record(stream)
     barrier()
     e2e_ms = rank_max(max(e2.elapsed_time(e3), (time.perf_counter() - t0) * 1e3))

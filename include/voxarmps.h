@@ -150,6 +150,15 @@ int mps_set_state(mps_ctx* ctx, const double* x, const double* y, const double* 
                   const double* u, const double* v, const double* w, const double* p);
 int mps_get_state(mps_ctx* ctx, double* x, double* y, double* z, double* u, double* v,
                   double* w, double* p);
+/* mps_set_state, mps_step and mps_get_state in one call: in[k] and out[k]
+ * are the caller-order host arrays of x y z u v w p (NULL skips one; in and
+ * out may be the same arrays).  The same results as the three calls; the
+ * copy of u, v, w, p runs on a second stream while the step's neighbour
+ * search runs, and they are applied after its reorder.  No counterpart in
+ * the reference, whose loop (main.cu:1027-1363) keeps the state in host
+ * arrays across steps: this is that loop's step with its host copies
+ * overlapped.  Returns mps_step's status bits with mps_get_state's. */
+int mps_step_io(mps_ctx* ctx, const double* const* in, double* const* out);
 /* Overwrite one state array between stage calls, host doubles in the caller's
  * particle order: x y z u v w (the packed copies the stages read follow),
  * p, pnew, un vn wn (the corrected velocity COLLISION2 and PREPDATA read),

@@ -43,7 +43,8 @@ EXPORTS = [
     "mps_pnd_star", "mps_bcon", "mps_pressure", "mps_phat", "mps_pressure_gradient",
     "mps_integrate", "mps_collision", "mps_commit", "mps_step", "mps_run", "mps_download",
     "mps_download_lists", "mps_get_scalar", "mps_get_error", "mps_last_message",
-    "mps_write_vtu", "mps_stream", "mps_set_state", "mps_get_state", "mps_set_field",
+    "mps_write_vtu", "mps_stream", "mps_set_state", "mps_get_state", "mps_step_io",
+    "mps_set_field",
     "mps_set_profile",
     "mps_cell_order_noalloc", "mps_set_scenes", "mps_set_graph",
     "mps_gnn_create", "mps_gnn_use", "mps_gnn_train", "mps_gnn_params", "mps_gnn_state",
@@ -100,6 +101,7 @@ def load_library(path: str = LIB_PATH):
     lib.mps_stream.restype = P
     lib.mps_set_state.argtypes = [P, P, P, P, P, P, P, P]
     lib.mps_get_state.argtypes = [P, P, P, P, P, P, P, P]
+    lib.mps_step_io.argtypes = [P, C.POINTER(P), C.POINTER(P)]
     lib.mps_set_field.argtypes = [P, C.c_char_p, DP]
     lib.mps_set_profile.argtypes = [P, C.c_int]
     lib.mps_set_graph.argtypes = [P, C.c_int]
@@ -273,6 +275,13 @@ class Solver:
     def set_state(self, *ptrs):
         """Host pointers (ints) for x, y, z, u, v, w, p in caller order; 0 skips."""
         return self._chk(self.lib.mps_set_state(self.h, *[p or None for p in ptrs]), "set_state")
+
+    def step_io(self, ins, outs):
+        """One step with the state in host arrays: ``ins`` and ``outs`` are 7
+        host pointers (ints; 0 skips) for x, y, z, u, v, w, p in caller order."""
+        a = (C.c_void_p * 7)(*[p or None for p in ins])
+        b = (C.c_void_p * 7)(*[p or None for p in outs])
+        return self._chk(self.lib.mps_step_io(self.h, a, b), "step_io")
 
     def set(self, name: str, values):
         """Overwrite one state array (caller order) between stage calls."""

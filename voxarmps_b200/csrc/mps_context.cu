@@ -60,10 +60,11 @@ int halloc(mps_ctx* c, T** p, size_t count)
 // Step graphs hold the buffer addresses they were captured with.
 void drop_graphs(mps_ctx* c)
 {
-    for (int k = 0; k < 2; k++) {
+    for (int k = 0; k < 4; k++) {
         if (c->gexec[k]) cudaGraphExecDestroy(c->gexec[k]);
         c->gexec[k] = nullptr;
         c->gkernels[k] = 0;
+        c->gdefer[k] = 0;
     }
 }
 
@@ -385,6 +386,28 @@ void vmps_drop_graphs(mps_ctx* c) { drop_graphs(c); }
 
 std::vector<void*>& vmps_reorder_alts(mps_ctx* ctx) { return ctx->alts; }
 
+// mps_step_io's deferred fields (bits 3..6 of state_defer: u, v, w, p; p also
+// sets pnew) from the staging area into the current cell order, after the
+// copies on the I/O stream have ended; then the packed velocities.  Inside a
+// step graph the wait is an external event node: each replay waits for the
+// copies recorded before its launch.
+int vmps_state_apply(mps_ctx* c)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    VMPS_CUDA(c, cudaStreamIsCapturing(c->stream, &cs));
+    VMPS_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_state,
+                                     cs == cudaStreamCaptureStatusActive ? cudaEventWaitExternal : 0));
+    double* dst[7] = {c->x, c->y, c->z, c->u, c->v, c->w, c->p};
+    StateIO io{};
+    for (int k = 3; k < 7; k++)
+        if (c->state_defer >> k & 1) io.f[k] = dst[k];
+    io.pnew = (c->state_defer >> 6 & 1) ? c->pnew : nullptr;
+    k_state_in<<<grid_blocks(c->n), kBlock, 0, c->stream>>>(c->n, c->pitch, c->oid, io,
+                                                            c->stage_io);
+    vmps_count_launch(1);
+    return vmps_pack_u(c);
+}
+
 // ------------------------------------------------------------------ C-ABI
 
 extern "C" {
@@ -424,6 +447,9 @@ int mps_destroy(mps_ctx* c)
     if (c->snap_ev) cudaEventDestroy(c->snap_ev);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->stream2) cudaStreamDestroy(c->stream2);
+    if (c->stream_io) cudaStreamDestroy(c->stream_io);
+    if (c->ev_io) cudaEventDestroy(c->ev_io);
+    if (c->ev_state) cudaEventDestroy(c->ev_state);
     delete c;
     return MPS_OK;
 }
@@ -696,7 +722,11 @@ static int enqueue_step(mps_ctx* c)
 // replayed afterwards; the CG loop inside is a conditional while node.
 static int graph_step(mps_ctx* c)
 {
-    const int par = (int)(c->swaps & 1);
+    const int par = (int)(c->swaps & 1) + (c->state_defer ? 2 : 0);
+    if (c->gexec[par] && c->gdefer[par] != c->state_defer) {  // another set of fields
+        cudaGraphExecDestroy(c->gexec[par]);
+        c->gexec[par] = nullptr;
+    }
     if (!c->stream2) VMPS_CUDA(c, cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
     TRY(vmps_gnn_prepare(c));  // no allocation inside the capture
     if (!c->gexec[par]) {
@@ -717,6 +747,7 @@ static int graph_step(mps_ctx* c)
         if (ie != cudaSuccess) c->gexec[par] = nullptr;
         VMPS_CUDA(c, ie);
         c->gkernels[par] = (long)(g_launches.load() - l0);
+        c->gdefer[par] = c->state_defer;
     } else {
         // the host side of a replay: the reorder's buffer exchange
         vmps_reorder_swap(c);
@@ -1017,6 +1048,49 @@ int mps_get_state(mps_ctx* c, double* x, double* y, double* z, double* u, double
                                          cudaMemcpyDeviceToHost, c->stream));
     VMPS_CUDA(c, cudaStreamSynchronize(c->stream));
     return MPS_OK;
+}
+
+int mps_step_io(mps_ctx* c, const double* const* in, double* const* out)
+{
+    NEED_INIT(c);
+    if (!in || !out) return MPS_ERR_ARG;
+    VMPS_CUDA(c, cudaSetDevice(c->device));
+    if (!c->stream_io) VMPS_CUDA(c, cudaStreamCreateWithFlags(&c->stream_io, cudaStreamNonBlocking));
+    if (!c->ev_io) VMPS_CUDA(c, cudaEventCreateWithFlags(&c->ev_io, cudaEventDisableTiming));
+    if (!c->ev_state) VMPS_CUDA(c, cudaEventCreateWithFlags(&c->ev_state, cudaEventDisableTiming));
+    const int n = c->n;
+    const long P = c->pitch;
+    const mps_config& f = c->cfg;
+    // the staging area is free once the context's stream has passed its
+    // earlier work
+    VMPS_CUDA(c, cudaEventRecord(c->ev_io, c->stream));
+    VMPS_CUDA(c, cudaStreamWaitEvent(c->stream_io, c->ev_io, 0));
+    double* dst[7] = {c->x, c->y, c->z, c->u, c->v, c->w, c->p};
+    StateIO pos{};
+    int defer = 0;
+    for (int k = 0; k < 7; k++) {
+        if (!in[k] || (f.dim == 2 && (k == 2 || k == 5))) continue;
+        // positions first on the context's stream (the neighbour search
+        // starts from them), the rest beside it
+        VMPS_CUDA(c, cudaMemcpyAsync(c->stage_io + k * P, in[k], sizeof(double) * n,
+                                     cudaMemcpyHostToDevice, k < 3 ? c->stream : c->stream_io));
+        if (k < 3) pos.f[k] = dst[k];
+        else defer |= 1 << k;
+    }
+    k_state_in<<<grid_blocks(n), kBlock, 0, c->stream>>>(n, P, c->oid, pos, c->stage_io);
+    vmps_count_launch(1);
+    // PNUM before the neighbour search reads the packed positions
+    if (f.method != 3 && !f.ppe_at_predicted) TRY(vmps_pack(c));
+    if (defer) VMPS_CUDA(c, cudaEventRecord(c->ev_state, c->stream_io));
+    c->state_defer = defer;
+    const int r = mps_step(c);
+    c->state_defer = 0;
+    if (r & (MPS_ERR_ARG | MPS_ERR_CUDA)) {
+        // the step stopped before taking the fields: leave no copy pending
+        cudaStreamSynchronize(c->stream_io);
+        return r;
+    }
+    return r | mps_get_state(c, out[0], out[1], out[2], out[3], out[4], out[5], out[6]);
 }
 
 int mps_set_profile(mps_ctx* c, int on)

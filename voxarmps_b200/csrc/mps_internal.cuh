@@ -152,9 +152,18 @@ struct mps_ctx {
     int ppe_warm = 1;  // initial guess of the last assembly (0: zero)
     // CUDA graph of one step per buffer parity (the reorder double-buffers
     // the persistent state, so the step's pointers alternate with period 2)
+    // (and per mps_step_io form: index parity + 2 when the step applies the
+    // velocities and pressure that mps_step_io copied in beside it)
     bool use_graph = false;
-    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
-    long gkernels[2] = {0, 0};
+    cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
+    long gkernels[4] = {0, 0, 0, 0};
+    int gdefer[4] = {0, 0, 0, 0};  // the deferred-field mask each graph applies
+    // mps_step_io: u, v, w, p travel on their own stream while the neighbour
+    // search runs and are applied after its reorder (bit k: field k of
+    // x, y, z, u, v, w, p; ev_state marks the end of their copies)
+    cudaStream_t stream_io = nullptr;
+    cudaEvent_t ev_io = nullptr, ev_state = nullptr;
+    int state_defer = 0;
     long swaps = 0;
     double cg_relres = 0;
     double cg_r0 = 0;  // relative residual of the CG starting point
@@ -491,4 +500,6 @@ int vmps_collision(mps_ctx* ctx);
 int vmps_commit(mps_ctx* ctx);
 int vmps_count_launch(int k);
 int vmps_pack(mps_ctx* ctx);
+int vmps_pack_u(mps_ctx* ctx);
+int vmps_state_apply(mps_ctx* ctx);
 int vmps_scan(mps_ctx* ctx, int m, const int* in, int* out);

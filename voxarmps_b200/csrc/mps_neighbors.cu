@@ -734,6 +734,12 @@ int vmps_neighbors(mps_ctx* ctx)
         ctx->lists_ms += ms;
         ctx->lists_launches++;
     }
+    // mps_step_io's velocities and pressure, copied while the lists were
+    // built, go into the new order (nothing above reads them)
+    if (ctx->state_defer) {
+        int r = vmps_state_apply(ctx);
+        if (r != MPS_OK) return r;
+    }
     VMPS_CUDA(ctx, cudaGetLastError());
     return MPS_OK;
 }

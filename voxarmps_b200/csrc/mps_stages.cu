@@ -1072,6 +1072,20 @@ int vmps_pack(mps_ctx* c)
     return MPS_OK;
 }
 
+// the packed velocities alone (mps_step_io's deferred velocities)
+int vmps_pack_u(mps_ctx* c)
+{
+    if (c->cfg.precision >= 1) {
+        k_pack_f<<<grid_blocks(c->n), kBlock, 0, c->stream>>>(c->n, c->u, c->v, c->w, 0.0, 0.0,
+                                                              0.0, nullptr, c->U4f);
+        vmps_count_launch(1);
+    }
+    k_pack<<<grid_blocks(c->n), kBlock, 0, c->stream>>>(c->n, c->u, c->v, c->w, nullptr, c->U4);
+    vmps_count_launch(1);
+    VMPS_CUDA(c, cudaGetLastError());
+    return MPS_OK;
+}
+
 int vmps_pnd(mps_ctx* c, int at_star, int correct, int which, double* out, bool track_max)
 {
     double re = which == 0 ? c->cfg.re_l : c->cfg.re_s;
