@@ -450,6 +450,8 @@ int mps_destroy(mps_ctx* c)
     if (c->stream_io) cudaStreamDestroy(c->stream_io);
     if (c->ev_io) cudaEventDestroy(c->ev_io);
     if (c->ev_state) cudaEventDestroy(c->ev_state);
+    for (auto e : c->ev_out)
+        if (e) cudaEventDestroy(e);
     delete c;
     return MPS_OK;
 }
@@ -1037,15 +1039,23 @@ int mps_get_state(mps_ctx* c, double* x, double* y, double* z, double* u, double
     const long P = c->pitch;
     double* out[7] = {x, y, z, u, v, w, p};
     double* from[7] = {c->x, c->y, c->z, c->u, c->v, c->w, c->p};
-    StateIO io{};
-    for (int k = 0; k < 7; k++)
-        if (out[k] && !(c->cfg.dim == 2 && (k == 2 || k == 5))) io.f[k] = from[k];
-    k_state_out<<<grid_blocks(n), kBlock, 0, c->stream>>>(n, P, c->oid, io, c->stage_io);
-    vmps_count_launch(1);
-    for (int k = 0; k < 7; k++)
-        if (io.f[k])
-            VMPS_CUDA(c, cudaMemcpyAsync(out[k], c->stage_io + k * P, sizeof(double) * n,
-                                         cudaMemcpyDeviceToHost, c->stream));
+    if (!c->stream_io) VMPS_CUDA(c, cudaStreamCreateWithFlags(&c->stream_io, cudaStreamNonBlocking));
+    // one field at a time: its permutation into caller order on the
+    // context's stream, its copy to the host on the I/O stream, so that each
+    // copy overlaps the next field's permutation
+    for (int k = 0; k < 7; k++) {
+        if (!out[k] || (c->cfg.dim == 2 && (k == 2 || k == 5))) continue;
+        if (!c->ev_out[k]) VMPS_CUDA(c, cudaEventCreateWithFlags(&c->ev_out[k], cudaEventDisableTiming));
+        StateIO io{};
+        io.f[k] = from[k];
+        k_state_out<<<grid_blocks(n), kBlock, 0, c->stream>>>(n, P, c->oid, io, c->stage_io);
+        vmps_count_launch(1);
+        VMPS_CUDA(c, cudaEventRecord(c->ev_out[k], c->stream));
+        VMPS_CUDA(c, cudaStreamWaitEvent(c->stream_io, c->ev_out[k], 0));
+        VMPS_CUDA(c, cudaMemcpyAsync(out[k], c->stage_io + k * P, sizeof(double) * n,
+                                     cudaMemcpyDeviceToHost, c->stream_io));
+    }
+    VMPS_CUDA(c, cudaStreamSynchronize(c->stream_io));
     VMPS_CUDA(c, cudaStreamSynchronize(c->stream));
     return MPS_OK;
 }

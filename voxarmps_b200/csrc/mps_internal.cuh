@@ -163,6 +163,7 @@ struct mps_ctx {
     // x, y, z, u, v, w, p; ev_state marks the end of their copies)
     cudaStream_t stream_io = nullptr;
     cudaEvent_t ev_io = nullptr, ev_state = nullptr;
+    cudaEvent_t ev_out[7] = {};  // mps_get_state: field k permuted, its copy may start
     int state_defer = 0;
     long swaps = 0;
     double cg_relres = 0;
