@@ -343,6 +343,7 @@ int allocate(mps_ctx* c)
     TRY(dalloc(c, &c->cg_part, c->cg_part_cap));
     TRY(dalloc(c, &c->cg_scal, 32));
     TRY(dalloc(c, &c->cg_flag, 4));
+    TRY(dalloc(c, &c->cg_bar, 4));
     TRY(dalloc(c, &c->d_err, 1));
     TRY(dalloc(c, &c->len_max, 2));
     TRY(dalloc(c, &c->d_max, 1));

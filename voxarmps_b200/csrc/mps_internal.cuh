@@ -241,6 +241,7 @@ struct mps_ctx {
     size_t cg_part_cap = 0;      // doubles in cg_part
     double* cg_scal = nullptr;   // device scalars (rz, bb, rr, ...)
     int* cg_flag = nullptr;      // [0] done, [1] iterations
+    unsigned int* cg_bar = nullptr;  // k_cg_loop's grid barrier: arrivals, monotonic per launch
     int* cg_flag_host = nullptr; // pinned
     double* red_host = nullptr;  // pinned scratch for scalars
     unsigned int* d_err = nullptr;

@@ -588,6 +588,132 @@ __global__ void k_cg_commit(double* scal, int* flag, int use_cond,
     if (use_cond) cudaGraphSetConditional(cond, flag[0] ? 0u : 1u);
 }
 
+// Grid-wide barrier of k_cg_loop (a cooperative launch: every block is
+// resident).  Thread 0 of each block adds its arrival to a counter that
+// grows by the grid size per barrier and waits for the count of this
+// barrier, at most kBarSpins polls (about a second); past that it sets
+// MPS_ERR_NOT_CONVERGED and the block reports failure, so a lost block ends
+// the solve instead of hanging the GPU.
+constexpr long kBarSpins = 1L << 24;
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& target, unsigned* err,
+                                             int* sh_ok)
+{
+    __syncthreads();
+    target += gridDim.x;
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        __threadfence();
+        atomicAdd(bar, 1u);
+        long spins = 0;
+        while (ld_acquire_u32(bar) < target) {
+            if (++spins > kBarSpins) {
+                set_error(err, MPS_ERR_NOT_CONVERGED);
+                ok = 0;
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+        *sh_ok = ok;
+    }
+    __syncthreads();
+    return *sh_ok != 0;
+}
+
+// The whole Jacobi-PCG loop in one cooperative launch, for systems small
+// enough that the loop's launches, not its bytes, set the time: each
+// iteration runs k_cg_spmv, k_cg_update, k_cg_direction and k_cg_commit's
+// work in that order with a grid barrier between them, over the same grid
+// and the same fixed-order block partials, so it takes the same steps with
+// the same bits as the four kernels.  The iteration state (r.z, the count)
+// lives in registers, identical in every block; block 0 commits it at the
+// end.  The barrier counter is zeroed before the launch.
+__global__ void __launch_bounds__(kRedThreads) k_cg_loop(CG A, double* __restrict__ x,
+        double* __restrict__ r, double* __restrict__ zv, double* __restrict__ p,
+        double* __restrict__ s, double* __restrict__ part, double* scal, int* flag, double tol2,
+        int maxit, unsigned* bar, unsigned* err)
+{
+    __shared__ double sh[33];
+    __shared__ int sh_ok;
+    if (flag[0]) return;
+    Grp<kRowG> q;
+    const long nwarps = (long)gridDim.x * blockDim.x / kRowG;
+    const int np = A.nparts;
+    double* part_ps = part + 4 * np;
+    const double bb = scal[S_BB];
+    double rz_old = scal[S_RZ];
+    int it = flag[1];
+    unsigned target = 0;
+    for (;;) {
+        // s = A p, partial p.s (k_cg_spmv)
+        double ps = 0;
+        for (long w = q.gid; w < A.n; w += nwarps) {
+            const int i = (int)w;
+            const int2 m = A.mrow[i];
+            double si = 0;
+            if (m.y >= 0) {
+                si = spmv_row(A, q, p, i, m.x, m.y);
+                if (q.lane == 0) ps += p[i] * si;
+            }
+            if (q.lane == 0) s[i] = si;
+        }
+        ps = block_sum(ps, sh);
+        if (threadIdx.x == 0) part_ps[blockIdx.x] = ps;
+        if (!grid_barrier(bar, target, err, &sh_ok)) return;
+        // x += alpha p, r -= alpha s, z = M^-1 r, partials r.z, r.r (k_cg_update)
+        const double alpha = rz_old / reduce_parts(part_ps, np, sh);
+        double rz = 0, rr = 0;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+            if (A.bcon[i] != 0) continue;
+            const double xi = x[i] + alpha * p[i];
+            const double ri = r[i] - alpha * s[i];
+            const double zi = A.precond ? ri / A.diag[i] : ri;
+            x[i] = xi;
+            r[i] = ri;
+            zv[i] = zi;
+            rz += ri * zi;
+            rr += ri * ri;
+        }
+        rz = block_sum(rz, sh);
+        rr = block_sum(rr, sh);
+        if (threadIdx.x == 0) {
+            part[blockIdx.x] = rz;
+            part[np + blockIdx.x] = rr;
+        }
+        if (!grid_barrier(bar, target, err, &sh_ok)) return;
+        // beta, the stop test, p = z + beta p (k_cg_direction, k_cg_commit)
+        const double rzn = reduce_parts(part, np, sh);
+        const double rrn = reduce_parts(part + np, np, sh);
+        const double beta = rzn / rz_old;
+        it++;
+        const bool done = rrn <= tol2 * bb || it >= maxit || !(rrn == rrn);
+        if (!done) {
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n;
+                 i += gridDim.x * blockDim.x)
+                if (A.bcon[i] == 0) p[i] = zv[i] + beta * p[i];
+        }
+        rz_old = rzn;
+        if (done) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                scal[S_RZ] = rzn;
+                scal[S_RR] = rrn;
+                flag[1] = it;
+                flag[0] = 1;
+            }
+            return;
+        }
+        if (!grid_barrier(bar, target, err, &sh_ok)) return;
+    }
+}
+
 // worst relative residual over batched scenes -> scal[S_WORST]
 __global__ void k_scene_worst(int nscenes, const double* __restrict__ sbb,
                               const double* __restrict__ srr, double* scal)
@@ -1022,13 +1148,43 @@ static int ppe_assemble(mps_ctx* c, int* warm_out, double* r0 = nullptr, bool* f
 // grid of the CG kernels: blocks per SM from the autotuner, else as many as
 // fit (at most 8); cg_part holds [0,3*nblk) start/update partials and
 // [4*nblk,5*nblk) p.s
-static int cg_grid(mps_ctx* c, int* out)
+// Systems of at most this many rows solve in k_cg_loop (FP64, one scene):
+// there the four launches per iteration and their gaps, not the bytes, set
+// the iteration's time.  Measured: the 2D dam of 1,928 particles 0.272
+// against 0.352 ms per step; the 86,118-particle two-phase scene 2.77
+// against 2.28 ms (three grid barriers per iteration over 592 blocks cost
+// more than the graph's kernel boundaries), the 1.6 M dam 27.1 against 20.3.
+constexpr int kLoopMaxRows = 16384;
+
+static bool use_cg_loop(mps_ctx* c)
+{
+    if (c->cfg.precision >= 1 || c->nscenes > 1 || c->n > kLoopMaxRows) return false;
+    int coop = 0;
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return coop != 0;
+}
+
+static int cg_grid(mps_ctx* c, int* out, bool loop = false)
 {
     int nblk = 0, occ = 0;
     VMPS_CUDA(c, cudaDeviceGetAttribute(&nblk, cudaDevAttrMultiProcessorCount, c->device));
     VMPS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg_spmv, kRedThreads, 0));
+    const int sms = nblk;
+    if (loop) {  // the cooperative loop needs its whole grid resident
+        int occ_loop = 0;
+        VMPS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_loop, k_cg_loop,
+                                                                   kRedThreads, 0));
+        occ = std::min(occ, occ_loop);
+    }
     const int bps = c->tune_cg_bps > 0 ? c->tune_cg_bps : 8;
     nblk *= std::max(1, std::min(occ, bps));
+    // the loop's barriers wait for every block: no more blocks than the
+    // rows' warps need, at least one per SM
+    if (loop) nblk = std::min(nblk, std::max(sms, (c->n + kRedThreads / kRowG - 1) /
+                                                      (kRedThreads / kRowG)));
     if ((size_t)5 * nblk > c->cg_part_cap) {
         c->msg = "CG partial buffer too small for the launch grid";
         return MPS_ERR_ARG;
@@ -1045,10 +1201,13 @@ int vmps_ppe(mps_ctx* c)
     const bool mixed = f.precision >= 1;
     int warm = 0, nblk = 0;
     bool fused = false;
+    // small systems: the loop in one cooperative launch, over a grid that
+    // the four-kernel loop (profiled runs) shares, so both give the same bits
+    const bool loop_grid = use_cg_loop(c);
     {
         int r = ppe_assemble(c, &warm, c->cg_r, &fused);
         if (r != MPS_OK) return r;
-        r = cg_grid(c, &nblk);
+        r = cg_grid(c, &nblk, loop_grid);
         if (r != MPS_OK) return r;
     }
     // zero initial guess (the assembly zeroed pnew): r = b exactly, so the
@@ -1064,27 +1223,30 @@ int vmps_ppe(mps_ctx* c)
     VMPS_CUDA(c, cudaStreamGetCaptureInfo(st, &cap, nullptr, &cgraph, nullptr, nullptr));
     const bool graph = cap == cudaStreamCaptureStatusActive;
     cudaGraphConditionalHandle cond = 0;
-    if (graph) VMPS_CUDA(c, cudaGraphConditionalHandleCreate(&cond, cgraph, 1, cudaGraphCondAssignDefault));
+    const bool loop = loop_grid && !c->profile;  // profiling times each SpMV launch
+    if (graph && !loop)
+        VMPS_CUDA(c, cudaGraphConditionalHandleCreate(&cond, cgraph, 1, cudaGraphCondAssignDefault));
+    const int use_cond = graph && !loop ? 1 : 0;
     IR I{c->mcv32, c->ir_d, c->ir_r, c->ir_z, c->ir_p, c->ir_s};
     if (mixed && fused) {
         k_ir_start_rows<<<nblk, kRedThreads, 0, st>>>(G, I, c->source, c->bcon, c->pnew, c->cg_r,
                                                       c->cg_part);
         k_ir_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal,
-                                                      c->cg_flag, graph ? 1 : 0, cond);
+                                                      c->cg_flag, use_cond, cond);
     } else if (mixed) {
         k_ir_start<<<nblk, kRedThreads, 0, st>>>(G, I, c->source, c->pnew, c->cg_r, c->cg_part);
         k_ir_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal,
-                                                      c->cg_flag, graph ? 1 : 0, cond);
+                                                      c->cg_flag, use_cond, cond);
     } else if (fused) {
         k_cg_start_rows<<<nblk, kRedThreads, 0, st>>>(G, c->source, c->bcon, c->pnew, c->cg_r,
                                                       c->cg_z, c->cg_p, c->cg_part);
         k_cg_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal,
-                                                      c->cg_flag, graph ? 1 : 0, cond);
+                                                      c->cg_flag, use_cond, cond);
     } else {
         k_cg_start<<<nblk, kRedThreads, 0, st>>>(G, c->source, c->pnew, c->cg_r, c->cg_z,
                                                  c->cg_p, c->cg_part);
         k_cg_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal,
-                                                      c->cg_flag, graph ? 1 : 0, cond);
+                                                      c->cg_flag, use_cond, cond);
     }
     vmps_count_launch(2);
     if (batched) {
@@ -1133,13 +1295,27 @@ int vmps_ppe(mps_ctx* c)
         k_cg_direction<<<nblk, kRedThreads, 0, s>>>(G, c->cg_z, c->cg_p, c->cg_part, c->cg_scal,
                                                     c->cg_flag, tol2, f.cg_max, c->nscenes,
                                                     c->sok);
-        k_cg_commit<<<1, 1, 0, s>>>(c->cg_scal, c->cg_flag, graph ? 1 : 0, cond);
+        k_cg_commit<<<1, 1, 0, s>>>(c->cg_scal, c->cg_flag, use_cond, cond);
         VMPS_CUDA(c, cudaGetLastError());
         return MPS_OK;
     };
     c->cg_loop_kernels = batched ? 5 : 4;
     c->cg_nspmv = 0;
-    if (graph) {
+    if (loop) {
+        VMPS_CUDA(c, cudaMemsetAsync(c->cg_bar, 0, sizeof(unsigned), st));
+        double* xp = c->pnew;
+        double *rp = c->cg_r, *zp = c->cg_z, *pp = c->cg_p, *sp = c->cg_s, *part = c->cg_part,
+               *scal = c->cg_scal;
+        int* flag = c->cg_flag;
+        int maxit = f.cg_max;
+        unsigned *bar = c->cg_bar, *err = c->d_err;
+        void* args[] = {&G, &xp, &rp, &zp, &pp, &sp, &part, &scal, &flag, &tol2, &maxit, &bar, &err};
+        VMPS_CUDA(c, cudaLaunchCooperativeKernel((const void*)k_cg_loop, dim3(nblk),
+                                                 dim3(kRedThreads), args, 0, st));
+        vmps_count_launch(1);
+        c->cg_loop_kernels = 0;
+        c->cg_nspmv = 1;
+    } else if (graph) {
         const cudaGraphNode_t* deps = nullptr;
         size_t ndeps = 0;
         VMPS_CUDA(c, cudaStreamGetCaptureInfo(st, &cap, nullptr, &cgraph, &deps, &ndeps));
