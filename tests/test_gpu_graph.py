@@ -94,3 +94,26 @@ def test_graph_off_again_and_reinit():
         assert np.array_equal(s.get(f), ref.get(f)), f
     s.close()
     ref.close()
+
+
+def test_cg_loop_equals_four_kernel_loop():
+    """The 2D dam's 1,928-row system solves in one cooperative launch
+    (k_cg_loop); profiled steps, which time every SpMV launch, run the four
+    kernels per iteration over the same grid and partials instead.  Both
+    give the same bits and iteration counts."""
+    cfg, case = config.baseline(0)
+    cfg = gpu_cfg(cfg)
+    runs = []
+    for profile in (False, True):
+        s = vm.Solver(cfg, case)
+        assert s.init() == 0
+        s.set_profile(profile)
+        iters = []
+        for _ in range(5):
+            assert s.step() == 0
+            iters.append(int(s.scalar("cg_iters")))
+        runs.append(({f: s.get(f) for f in ("x", "y", "u", "v", "p", "pnew")}, iters))
+        s.close()
+    for f in runs[0][0]:
+        assert np.array_equal(runs[0][0][f].view(np.uint64), runs[1][0][f].view(np.uint64)), f
+    assert runs[0][1] == runs[1][1]
