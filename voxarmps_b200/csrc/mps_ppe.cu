@@ -33,6 +33,12 @@ constexpr int kRedThreads = 256;
 // warp per row (16 or 8 lanes: 0.69 ms against 0.61 ms per launch); the
 // assembly runs 16 lanes per row (PPE stage 12.4 ms against 12.8 ms at 32)
 constexpr int kRowG = 32;
+// systems of at most this many rows run their FP64 products with 16 lanes
+// per row (two rows per warp): the 86,118-particle two-phase scene 2.04
+// against 2.38 ms per step (rows of ~50 entries leave a warp's second half
+// idle, and two rows per warp halve each warp's chain of dependent rows);
+// the 1.6 M-particle dam keeps whole warps (0.61 against 0.69 ms per SpMV)
+constexpr int kNarrowMaxRows = 262144;
 constexpr int kAsmG = 16;
 // lanes per row of the mixed-precision products (inner FP32 and refinement):
 // 16 (config 2 at 19.37 ms/step against 19.63 ms with 32 or 8 lanes)
@@ -311,8 +317,8 @@ __device__ __forceinline__ double spmv_row(const CG& A, const Grp<G>& q,
     return A.diag[i] * (double)v[i] + acc;
 }
 
-template <typename V>
-__device__ __forceinline__ double spmv_row_warp(const CG& A, const Grp<kRowG>& q,
+template <typename V, int G = kRowG>
+__device__ __forceinline__ double spmv_row_warp(const CG& A, const Grp<G>& q,
                                                 const V* __restrict__ v, int i)
 {
     return spmv_row(A, q, v, i, A.moff[i], A.mlen[i]);
@@ -354,13 +360,14 @@ __device__ __forceinline__ float spmv_row_warp32(const CG& A, const int2* __rest
 // r = b - A x, z = M^-1 r, p = z; partials of b.b, r.z, r.r
 // 8 resident blocks per SM (32 registers): the grid is 8 blocks per SM and
 // every block must be resident, or a second wave doubles the time
+template <int G>
 __global__ void __launch_bounds__(256, 8) k_cg_start(CG A, const double* __restrict__ b, const double* __restrict__ x,
                            double* __restrict__ r, double* __restrict__ zv, double* __restrict__ p,
                            double* __restrict__ part)
 {
     __shared__ double sh[33];
-    Grp<kRowG> q;
-    const long nwarps = (long)gridDim.x * blockDim.x / kRowG;
+    Grp<G> q;
+    const long nwarps = (long)gridDim.x * blockDim.x / G;
     double bb = 0, rz = 0, rr = 0;
     for (long w = q.gid; w < A.n; w += nwarps) {
         int i = (int)w;
@@ -452,14 +459,16 @@ __global__ void k_cg_start_scalars(int nparts, const double* __restrict__ part, 
     }
 }
 
-// s = A p and partial p.s; one warp per row
+// s = A p and partial p.s; G lanes per row (a whole warp, or half of one
+// for the systems of up to kNarrowMaxRows rows)
+template <int G>
 __global__ void k_cg_spmv(CG A, const double* __restrict__ p, double* __restrict__ s,
                           double* __restrict__ part, const int* __restrict__ flag)
 {
     __shared__ double sh[33];
     if (flag[0]) return;
-    Grp<kRowG> q;
-    const long nwarps = (long)gridDim.x * blockDim.x / kRowG;
+    Grp<G> q;
+    const long nwarps = (long)gridDim.x * blockDim.x / G;
     double ps = 0;
     // one 8-byte load of (offset, length) per row; length -1 marks rows
     // outside the system (measured 0.569 against 0.574 ms per launch with
@@ -636,6 +645,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& target, un
 // the same bits as the four kernels.  The iteration state (r.z, the count)
 // lives in registers, identical in every block; block 0 commits it at the
 // end.  The barrier counter is zeroed before the launch.
+template <int G>
 __global__ void __launch_bounds__(kRedThreads) k_cg_loop(CG A, double* __restrict__ x,
         double* __restrict__ r, double* __restrict__ zv, double* __restrict__ p,
         double* __restrict__ s, double* __restrict__ part, double* scal, int* flag, double tol2,
@@ -644,8 +654,8 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_loop(CG A, double* __restric
     __shared__ double sh[33];
     __shared__ int sh_ok;
     if (flag[0]) return;
-    Grp<kRowG> q;
-    const long nwarps = (long)gridDim.x * blockDim.x / kRowG;
+    Grp<G> q;
+    const long nwarps = (long)gridDim.x * blockDim.x / G;
     const int np = A.nparts;
     double* part_ps = part + 4 * np;
     const double bb = scal[S_BB];
@@ -1167,24 +1177,24 @@ static bool use_cg_loop(mps_ctx* c)
     return coop != 0;
 }
 
-static int cg_grid(mps_ctx* c, int* out, bool loop = false)
+static int cg_grid(mps_ctx* c, int* out, bool loop = false, int g = kRowG)
 {
     int nblk = 0, occ = 0;
     VMPS_CUDA(c, cudaDeviceGetAttribute(&nblk, cudaDevAttrMultiProcessorCount, c->device));
-    VMPS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg_spmv, kRedThreads, 0));
+    VMPS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                     &occ, g == 16 ? k_cg_spmv<16> : k_cg_spmv<kRowG>, kRedThreads, 0));
     const int sms = nblk;
     if (loop) {  // the cooperative loop needs its whole grid resident
         int occ_loop = 0;
-        VMPS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_loop, k_cg_loop,
-                                                                   kRedThreads, 0));
+        VMPS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                         &occ_loop, g == 16 ? k_cg_loop<16> : k_cg_loop<kRowG>, kRedThreads, 0));
         occ = std::min(occ, occ_loop);
     }
     const int bps = c->tune_cg_bps > 0 ? c->tune_cg_bps : 8;
     nblk *= std::max(1, std::min(occ, bps));
     // the loop's barriers wait for every block: no more blocks than the
     // rows' warps need, at least one per SM
-    if (loop) nblk = std::min(nblk, std::max(sms, (c->n + kRedThreads / kRowG - 1) /
-                                                      (kRedThreads / kRowG)));
+    if (loop) nblk = std::min(nblk, std::max(sms, (c->n + kRedThreads / g - 1) / (kRedThreads / g)));
     if ((size_t)5 * nblk > c->cg_part_cap) {
         c->msg = "CG partial buffer too small for the launch grid";
         return MPS_ERR_ARG;
@@ -1204,10 +1214,11 @@ int vmps_ppe(mps_ctx* c)
     // small systems: the loop in one cooperative launch, over a grid that
     // the four-kernel loop (profiled runs) shares, so both give the same bits
     const bool loop_grid = use_cg_loop(c);
+    const bool narrow = n <= kNarrowMaxRows;  // 16 lanes per row in the FP64 products
     {
         int r = ppe_assemble(c, &warm, c->cg_r, &fused);
         if (r != MPS_OK) return r;
-        r = cg_grid(c, &nblk, loop_grid);
+        r = cg_grid(c, &nblk, loop_grid, narrow ? 16 : kRowG);
         if (r != MPS_OK) return r;
     }
     // zero initial guess (the assembly zeroed pnew): r = b exactly, so the
@@ -1243,7 +1254,8 @@ int vmps_ppe(mps_ctx* c)
         k_cg_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal,
                                                       c->cg_flag, use_cond, cond);
     } else {
-        k_cg_start<<<nblk, kRedThreads, 0, st>>>(G, c->source, c->pnew, c->cg_r, c->cg_z,
+        (narrow ? k_cg_start<16> : k_cg_start<kRowG>)<<<nblk, kRedThreads, 0, st>>>(
+            G, c->source, c->pnew, c->cg_r, c->cg_z,
                                                  c->cg_p, c->cg_part);
         k_cg_start_scalars<<<1, kRedThreads, 0, st>>>(nblk, c->cg_part, tol2, c->cg_scal,
                                                       c->cg_flag, use_cond, cond);
@@ -1282,7 +1294,8 @@ int vmps_ppe(mps_ctx* c)
             VMPS_CUDA(c, cudaGetLastError());
             return MPS_OK;
         }
-        k_cg_spmv<<<nblk, kRedThreads, 0, s>>>(G, c->cg_p, c->cg_s, c->cg_part + 4 * nblk,
+        (narrow ? k_cg_spmv<16> : k_cg_spmv<kRowG>)<<<nblk, kRedThreads, 0, s>>>(
+            G, c->cg_p, c->cg_s, c->cg_part + 4 * nblk,
                                                c->cg_flag);
         if (c->profile && !graph) VMPS_CUDA(c, cudaEventRecord(c->ev_spmv[2 * k + 1], s));
         k_cg_update<<<nblk, kRedThreads, 0, s>>>(G, c->pnew, c->cg_r, c->cg_z, c->cg_p, c->cg_s,
@@ -1310,7 +1323,8 @@ int vmps_ppe(mps_ctx* c)
         int maxit = f.cg_max;
         unsigned *bar = c->cg_bar, *err = c->d_err;
         void* args[] = {&G, &xp, &rp, &zp, &pp, &sp, &part, &scal, &flag, &tol2, &maxit, &bar, &err};
-        VMPS_CUDA(c, cudaLaunchCooperativeKernel((const void*)k_cg_loop, dim3(nblk),
+        const void* fn = narrow ? (const void*)k_cg_loop<16> : (const void*)k_cg_loop<kRowG>;
+        VMPS_CUDA(c, cudaLaunchCooperativeKernel(fn, dim3(nblk),
                                                  dim3(kRedThreads), args, 0, st));
         vmps_count_launch(1);
         c->cg_loop_kernels = 0;
@@ -1510,7 +1524,7 @@ int mps_dcg_start(mps_ctx* c, double* local3)
     if (r != MPS_OK) return r;
     const CG G = dcg_args(c, nblk);
     VMPS_CUDA(c, cudaMemsetAsync(c->cg_flag, 0, 4 * sizeof(int), c->stream));
-    k_cg_start<<<nblk, kRedThreads, 0, c->stream>>>(G, c->source, c->pnew, c->cg_r, c->cg_z,
+    k_cg_start<kRowG><<<nblk, kRedThreads, 0, c->stream>>>(G, c->source, c->pnew, c->cg_r, c->cg_z,
                                                      c->cg_p, c->cg_part);
     vmps_count_launch(1);
     return local_sums_to_host(c, nblk, c->cg_part, 3, local3);  // b.b, r.z, r.r
@@ -1524,7 +1538,7 @@ int mps_dcg_spmv(mps_ctx* c, double* local_ps)
     int r = cg_grid(c, &nblk);
     if (r != MPS_OK) return r;
     const CG G = dcg_args(c, nblk);
-    k_cg_spmv<<<nblk, kRedThreads, 0, c->stream>>>(G, c->cg_p, c->cg_s, c->cg_part + 4 * nblk,
+    k_cg_spmv<kRowG><<<nblk, kRedThreads, 0, c->stream>>>(G, c->cg_p, c->cg_s, c->cg_part + 4 * nblk,
                                                     c->cg_flag);
     vmps_count_launch(1);
     return local_sums_to_host(c, nblk, c->cg_part + 4 * nblk, 1, local_ps);
